@@ -1,0 +1,196 @@
+/*
+ * swehr.h -- C ABI of the B200-native SWEHR time step.
+ *
+ * The reference (SWEHR.c of csdms-contrib/swehr) is one C program whose
+ * solver is the body of `while (t<tend)` inside main() (SWEHR.c:808-1699).
+ * It has no library interface; the entry points below are the seam a
+ * maintainer would cut at, each one citing the region of SWEHR.c it
+ * replaces.  All pointers are plain host pointers; the library copies what
+ * it is given and never keeps a caller buffer.  No torch or CUDA types
+ * appear in the signatures.
+ *
+ * Grid orientation follows the reference: i = 1..nx is the first index,
+ * j = 1..ny the second, and every nx*ny host array is i-major with j
+ * contiguous, element (i,j) at [(i-1)*ny + (j-1)] -- the order topoin.txt is
+ * read in (SWEHR.c:223-227).
+ */
+#ifndef SWEHR_H
+#define SWEHR_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define SWEHR_ABI_VERSION 1
+#define SWEHR_MAX_CLASSES 16
+
+typedef enum swehr_status {
+    SWEHR_OK = 0,
+    SWEHR_CFL_ERROR = 1,    /* Courant number > 1 (SWEHR.c:1412-1413); the step completes, then stepping stops */
+    SWEHR_NAN = 2,          /* non-finite water depth detected (only when params.stop_on_nan) */
+    SWEHR_TIMEOUT = 3,      /* host wall-clock limit of swehr_advance reached */
+    SWEHR_CUDA_ERROR = 4,   /* a CUDA runtime call failed; see swehr_last_error() */
+    SWEHR_INVALID = 5,      /* bad argument (sizes, NULL pointers, class count, ...) */
+    SWEHR_OOM = 6,          /* device allocation failed / pool budget exceeded */
+    SWEHR_NO_DEVICE = 7,    /* no CUDA device visible */
+    SWEHR_BUSY = 8          /* pool: no slot or memory free right now */
+} swehr_status;
+
+typedef enum swehr_precision {
+    SWEHR_FP64 = 0,         /* plain form: every operation in FP64, bit-identical to the CPU restatement */
+    SWEHR_MIXED = 1         /* FP32 bulk; FP64 for z, cumulative infiltration, deposited mass and budgets */
+} swehr_precision;
+
+/* Run parameters.  The first block is input.txt in file order
+ * (SWEHR.c:474-504); everything after it is hard-coded in the reference and
+ * exposed here with the reference's values as defaults (swehr_params_default). */
+typedef struct swehr_params {
+    /* input.txt: nx ny dx F manning0 tend a ad h0 mtstar0 rnum rint sclass J */
+    int32_t nx, ny;
+    double  dx;
+    double  F;              /* effective fraction of stream power in entrainment */
+    double  manning0;       /* read but unused by the reference (roughness is hard-coded) */
+    double  tend;           /* total simulated time [s] */
+    double  a, ad;          /* detachability of original / deposited soil */
+    double  h0;             /* critical depth in rain-splash depth dependence */
+    double  mtstar0;        /* deposited mass that fully shields the soil */
+    int32_t rnum;           /* number of hyetograph entries */
+    int32_t sclass;         /* number of sediment size classes S */
+    double  rint;           /* seconds per hyetograph entry */
+    double  J;              /* energy to entrain a unit mass */
+    /* SWEHR.c:490-494 */
+    double  hcfriction, depthdependentexponent, b, af, afr;
+    /* SWEHR.c:632-633 */
+    double  cstable, maxstep;
+    /* SWEHR.c:638-650 */
+    double  g, hfilm, phi, rhos, rhow, nu, frictionangle, cohesion, lambda, cthreshold, betabedload;
+    /* per-cell soil defaults, SWEHR.c:236-246 (uniform unless a per-cell array is given) */
+    double  roughness, ks, theta0, thetas, hf, vinf0, uc, uc2;
+    /* boundary types BNDRY[1..4] = {i=1, j=1, i=nx, j=ny} (SWEHR.c:617-621): 0 transmissive, 1 solid */
+    int32_t bndry[4];
+    int32_t inflow;         /* 1: hard-wired sediment-laden inflow ghost at j=ny (SWEHR.c:1010-1035) */
+    int32_t stop_on_nan;    /* 1: stop with SWEHR_NAN when a non-finite depth appears */
+    /* stage / point series (SWEHR.c:1593-1676): stageint [s], outlet row, six sample points (1-based) */
+    double  stageint;
+    int32_t outlet_row;
+    int32_t npoints;
+    int32_t xpoint[6], ypoint[6];
+    /* moving Gaussian storm (an extension; the reference only has a uniform hyetograph).
+     * When storm_peak > 0 the rain at cell centre (x,y) = ((i-0.5)dx, (j-0.5)dx) is
+     * storm_peak*exp(-0.5*((x-x0-vx t)^2+(y-y0-vy t)^2)/storm_radius^2) and the hyetograph is ignored. */
+    double  storm_peak, storm_radius, storm_x0, storm_y0, storm_vx, storm_vy;
+    int32_t budget;         /* 1: accumulate compensated water / sediment budget terms every step */
+    int32_t reserved_i[7];
+    double  reserved_d[8];
+} swehr_params;
+
+/* Host inputs (copied by swehr_create). */
+typedef struct swehr_inputs {
+    const double *topo;     /* nx*ny elevations, i-major (topoin.txt) */
+    const double *rain;     /* rnum rates [m/s] (rain.txt) */
+    const double *ds;       /* sclass diameters [m] (particlesizein.txt) */
+    const double *pfrac;    /* sclass mass fractions of the original soil (particlepercentin.txt) */
+    const double *ks;       /* optional nx*ny saturated conductivity [m/s]; NULL -> params.ks everywhere */
+} swehr_inputs;
+
+/* Fields readable with swehr_read_field; all are nx*ny, i-major. */
+typedef enum swehr_field {
+    SWEHR_FIELD_H = 0,        /* U[1]  depth            (depth.txt) */
+    SWEHR_FIELD_HU = 1,       /* U[2]                   (uh.txt) */
+    SWEHR_FIELD_HV = 2,       /* U[3]                   (vh.txt) */
+    SWEHR_FIELD_Z = 3,        /* TOPO                   (topoout.txt) */
+    SWEHR_FIELD_VINF = 4,     /* cumulative infiltration */
+    SWEHR_FIELD_U = 5,        /* U[3+k] suspended mass per area, class k (ch.txt for k=1) */
+    SWEHR_FIELD_M = 6,        /* M[k] deposited mass per area, class k */
+    SWEHR_FIELD_TOTM = 7,     /* TOTM                   (m.txt) */
+    SWEHR_FIELD_TOTSED = 8,   /* TOTSED                 (c.txt) */
+    SWEHR_FIELD_VEL = 9,      /* |v|                    (vel.txt) */
+    SWEHR_FIELD_MAXVEL = 10,  /*                        (maxvel.txt) */
+    SWEHR_FIELD_MAXDEPTH = 11,/*                        (maxdepth.txt) */
+    SWEHR_FIELD_DEP = 12,     /* DEP deposited thickness */
+    SWEHR_FIELD_SED = 13      /* SED[k] suspended concentration, class k */
+} swehr_field;
+
+/* Progress of one swehr_advance call. */
+typedef struct swehr_progress {
+    double  t;              /* simulated time after the last completed step */
+    double  dt;             /* last time step */
+    double  courant;        /* last Courant number */
+    double  rain;           /* last uniform rain rate */
+    int64_t steps;          /* steps completed since swehr_create */
+    int64_t steps_this_call;
+    double  device_ms;      /* device time of this call, CUDA events on the context stream */
+    double  kernel_ms;      /* summed device time of the update kernel (only with swehr_set_timing(ctx,1)) */
+    int64_t kernel_launches;/* kernels this call launched */
+    int32_t status;
+    int32_t done;           /* 1 when t >= tend */
+} swehr_progress;
+
+/* Water / sediment budget (an addition; the reference keeps none).  All sums
+ * are over the interior cells in depth units [m] (water) or mass per area
+ * [kg/m^2] (sediment, per class), accumulated in compensated FP64.
+ * water:  sum(h+VINF)_now - sum(h+VINF)_0 == rain_in - outflow + clamp_gain + bulking
+ * sed k:  sum(U_k+M_k)_now - sum(U_k+M_k)_0 == detach_k - sed_outflow_k */
+typedef struct swehr_budget {
+    double water_now, water_init;
+    double rain_in, outflow, clamp_gain, bulking, infiltration;
+    double water_residual;                /* (now - init) - (rain_in - outflow + clamp_gain + bulking) */
+    double sed_now[SWEHR_MAX_CLASSES], sed_init[SWEHR_MAX_CLASSES];
+    double detach[SWEHR_MAX_CLASSES], sed_outflow[SWEHR_MAX_CLASSES];
+    double sed_residual[SWEHR_MAX_CLASSES];
+    int32_t sclass;
+    int32_t valid;
+} swehr_budget;
+
+typedef struct swehr_ctx swehr_ctx;
+
+/* Reference defaults for every parameter (SWEHR.c:490-494, 617-650, 236-246);
+ * input.txt values are zeroed and must be filled by the caller. */
+void swehr_params_default(swehr_params *p);
+size_t swehr_params_size(void);
+int swehr_abi_version(void);
+const char *swehr_status_str(int status);
+const char *swehr_last_error(void);
+
+/* Replaces SWEHR.c:540-803 (allocation, initialcondition, masks, neighbour
+ * tables, initial slopes and gravity).  Copies inputs to the device. */
+int swehr_create(const swehr_params *p, const swehr_inputs *in, int precision, swehr_ctx **out);
+
+/* Replaces the body of `while (t<tend)` (SWEHR.c:808-1591): steps until
+ * t >= min(t_stop, tend) or max_steps steps (max_steps < 0: unbounded) were
+ * taken.  dt is clamped against tend only (SWEHR.c:1411), so pausing at
+ * t_stop never changes the trajectory.  progress may be NULL. */
+int swehr_advance(swehr_ctx *ctx, double t_stop, int64_t max_steps, swehr_progress *progress);
+
+/* Replaces the final writers (SWEHR.c:1718-1747): copies one field (class k,
+ * 1-based, for the per-class fields) into dst[nx*ny], i-major, FP64. */
+int swehr_read_field(swehr_ctx *ctx, int field, int k, double *dst);
+
+/* Replaces STAGE / SAVEFLOW (SWEHR.c:1593-1676, written at 1749-1761).
+ * Copies up to max_rows rows of the stage series (24 doubles per row) and the
+ * point series (18 doubles per row, three per point) recorded so far;
+ * returns the row count through *rows. */
+int swehr_read_series(swehr_ctx *ctx, double *stage, double *saveflow, int64_t max_rows, int64_t *rows);
+
+/* Budget sums accumulated so far (requires params.budget = 1). */
+int swehr_get_budget(swehr_ctx *ctx, swehr_budget *b);
+
+/* 1: time the update kernel with CUDA events around every launch. */
+int swehr_set_timing(swehr_ctx *ctx, int on);
+
+/* Replaces nothing in the reference: uploads a whole state (one field) to
+ * continue from a snapshot; same layout as swehr_read_field. */
+int swehr_write_field(swehr_ctx *ctx, int field, int k, const double *src);
+
+/* Device bytes held by a context for the given sizes (admission control). */
+size_t swehr_footprint_bytes(int nx, int ny, int sclass, int precision);
+
+void swehr_destroy(swehr_ctx *ctx);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* SWEHR_H */
