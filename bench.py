@@ -1,0 +1,310 @@
+"""Benchmark of the SWEHR time step on B200.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl {swehr,reference}]
+
+Workload (N=1): the roofline domain -- 4096 x 4096 cells, dx = 2 m,
+diamond-square topography (Hurst 0.8, 40 m relief, seed 1) tilted 3 % toward
+i=1, uniform rain from a seeded 30-entry hyetograph, lognormal per-cell Ks,
+7 sediment classes -- run in the plain FP64 form.  A "step" is one SWEHR time
+step over the whole domain.  W untimed steps, then exactly K timed steps
+(the run continues the same trajectory); the 4096^2 state (6.7 GB) is far
+larger than L2, so no flush is needed between steps.
+
+N > 1 (torchrun): every rank advances its own replica of the domain (weak
+scaling, no data-path collective -- independent domains do not exchange
+anything); rank 0 prints the whole-job cell-steps/s from the max over ranks
+of the device-timed region.
+
+--impl reference: the reference program (SWEHR.c built by oracle/build_ref.py
+with its own OpenMP pragmas on) on a crop of the same domain, all host
+threads, timed by its own loop timer; rank 0 only.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+import numpy as np  # noqa: E402
+
+PEAKS_PATH = os.path.join(ROOT, "MEASURED_PEAKS.json")
+FALLBACK_HBM = 6650.0
+
+
+def algo_bytes_f64(S: int) -> int:
+    """Algorithmic bytes per cell-step of the plain FP64 form: every prognostic
+    field (h hu hv z VINF MAXDEPTH MAXVEL, U_k, M_k) read and written once,
+    plus the per-cell Ks read."""
+    return 16 * (7 + 2 * S) + 8
+
+
+def hbm_peak():
+    try:
+        with open(PEAKS_PATH) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    except Exception:
+        return FALLBACK_HBM, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clock samples during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.path = tempfile.mktemp(prefix="clocks_", suffix=".csv")
+        self.idx = gpu_index
+        self.proc = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.idx}", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        try:
+            for line in open(self.path):
+                p = [x.strip() for x in line.split(",")]
+                if len(p) < 9:
+                    continue
+                try:
+                    sm.append(float(p[1]))
+                    smax.append(float(p[2]))
+                except ValueError:
+                    continue
+                for n, v in zip(names, p[5:9]):
+                    if v.lower() in ("active", "1", "yes"):
+                        reasons.add(n)
+        except FileNotFoundError:
+            pass
+        try:
+            os.unlink(self.path)
+        except OSError:
+            pass
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(smax) if smax else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def bench_workload(args):
+    from swehr_b200 import workloads as W
+    return W.fractal_domain(nx=args.nx, ny=args.ny, dx=2.0, seed=1, steps=args.warmup + args.steps)
+
+
+def run_cpu_reference(case, crop: int, steps: int, threads: int):
+    """The reference program (OpenMP build) on a crop x crop corner of the
+    case for `steps` steps; returns (cell-steps/s, elapsed, threads)."""
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    import harness
+    from swehr_b200.workloads import Case
+    p = dict(case.params)
+    p["nx"], p["ny"] = crop, crop
+    sub = Case(case.name + f"_crop{crop}", p, case.topo[:crop, :crop].copy(), case.rain, case.ds, case.pfrac,
+               ks=None if case.ks is None else case.ks[:crop, :crop].copy())
+    if not os.path.exists(harness.ref_binary(True)):
+        raise FileNotFoundError("oracle/_ref/swehr_ref_omp not built")
+    _, out = harness.run_reference(sub, max_steps=steps, omp=True, threads=threads, dump=False, timeout=900)
+    for line in out.splitlines():
+        if line.startswith("SWEHR_REF"):
+            f = line.split()
+            n, el, th = int(f[2]), float(f[4]), int(f[6])
+            return crop * crop * n / el, el, th, n
+    raise RuntimeError("reference printed no timing line")
+
+
+def host_threads() -> int:
+    try:
+        return len(os.sched_getaffinity(0))
+    except Exception:
+        return os.cpu_count() or 1
+
+
+def reference_arm(args, rank: int):
+    if rank != 0:
+        return
+    case = bench_workload(args)
+    threads = host_threads()
+    # one timed "step" = one reference time step on a crop sized so K steps take ~1-2 minutes
+    budget_cell_steps = 1.5e8
+    crop = int(max(64, min(1024, (budget_cell_steps / max(args.steps, 1)) ** 0.5)))
+    try:
+        value, el, th, n = run_cpu_reference(case, crop, args.steps, threads)
+    except Exception as e:  # noqa: BLE001
+        print(json.dumps({"impl": "reference", "unavailable": f"reference program not runnable: {e}"}))
+        return
+    line = {
+        "impl": "reference", "metric": "cell-steps/s", "value": value, "unit": "cell-steps/s", "n_gpus": args.gpus,
+        "steps": n, "warmup": 0, "ms_per_step": el * 1e3 / max(n, 1), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded)",
+        "config": {"workload": f"fractal {args.nx}x{args.ny} dx=2 S=7, plain FP64; reference run on a "
+                               f"{crop}x{crop} crop of the same domain", "threads": th},
+        "cpu_baseline": {"value": value, "unit": "cell-steps/s", "cores": th, "kind": "reference",
+                         "sample": f"SWEHR.c (OpenMP pragmas on) on a {crop}x{crop} crop, {n} steps"},
+        "e2e": {"value": value, "unit": "cell-steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line))
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=2000)
+    ap.add_argument("--warmup", type=int, default=10)
+    ap.add_argument("--impl", default="swehr", choices=["swehr", "reference"])
+    ap.add_argument("--nx", type=int, default=4096)
+    ap.add_argument("--ny", type=int, default=4096)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        vis = os.environ.get("CUDA_VISIBLE_DEVICES")
+        devs = vis.split(",") if vis else [str(i) for i in range(64)]
+        os.environ["CUDA_VISIBLE_DEVICES"] = devs[local]
+
+    if args.impl == "reference":
+        reference_arm(args, rank)
+        return
+
+    dist = None
+    if world > 1:
+        import datetime
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(0)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+
+    from swehr_b200.lib import Simulation
+    case = bench_workload(args)
+    S = case.sclass
+    cells = case.cells()
+    sim = Simulation(case)
+    sim.advance(max_steps=args.warmup)
+
+    def barrier():
+        if dist is not None:
+            import torch
+            t = torch.ones(1, device="cuda")
+            dist.all_reduce(t)
+            torch.cuda.synchronize()
+
+    clocks = ClockSampler(local)
+    barrier()
+    clocks.start()
+    sim.set_timing(True)
+    pr = sim.advance(max_steps=args.steps)
+    sim.set_timing(False)
+    clk = clocks.stop()
+    barrier()
+    elapsed_ms = pr.device_ms
+    kernel_ms = pr.kernel_ms
+    steps_done = pr.steps_this_call
+    if dist is not None:
+        import torch
+        t = torch.tensor([elapsed_ms], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        elapsed_ms = float(t.item())
+    value = world * cells * steps_done / (elapsed_ms / 1e3)
+    sim.close()
+
+    # end-to-end through the C ABI from host buffers: create (H2D of every
+    # input) + the same steps + D2H of every output field, wall-clock
+    e2e = None
+    if not args.no_e2e:
+        barrier()
+        t0 = time.perf_counter()
+        s2 = Simulation(case)
+        s2.advance(max_steps=args.warmup + args.steps)
+        out = s2.fields()
+        t1 = time.perf_counter()
+        s2.close()
+        h2d = case.topo.nbytes + (case.ks.nbytes if case.ks is not None else 0) + case.rain.nbytes
+        d2h = sum(v.nbytes for v in out.values())
+        e2e_val = cells * (args.warmup + args.steps) / (t1 - t0)
+        if dist is not None:
+            import torch
+            t = torch.tensor([t1 - t0], device="cuda", dtype=torch.float64)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            e2e_val = world * cells * (args.warmup + args.steps) / float(t.item())
+        n_e2e = args.warmup + args.steps
+        e2e = {"value": e2e_val, "unit": "cell-steps/s", "h2d_bytes_per_step": h2d / n_e2e,
+               "d2h_bytes_per_step": d2h / n_e2e,
+               "scope": "swehr_create + swehr_advance + swehr_read_field of every output, host buffers"}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        try:
+            v, el, th, n = run_cpu_reference(case, 1024, 8, host_threads())
+            cpu = {"value": v, "unit": "cell-steps/s", "cores": th, "kind": "reference",
+                   "sample": f"SWEHR.c with its OpenMP pragmas on, 1024x1024 corner of the same domain, "
+                             f"first {n} steps, {el:.1f} s"}
+        except Exception as e:  # noqa: BLE001
+            cpu = {"value": None, "unit": "cell-steps/s", "cores": host_threads(), "kind": "reference",
+                   "sample": f"unavailable: {e}"}
+
+    if rank == 0:
+        peak, peak_kind = hbm_peak()
+        B = algo_bytes_f64(S)
+        upd_ms = kernel_ms / max(steps_done, 1)
+        achieved = B * cells / (upd_ms / 1e3) / 1e9 if upd_ms > 0 else None
+        traffic = None
+        tpath = os.path.join(ROOT, "profiles", "update_f64_traffic.json")
+        if os.path.exists(tpath):
+            try:
+                traffic = json.load(open(tpath)).get("bytes_per_launch_scaled")
+            except Exception:
+                traffic = None
+        line = {
+            "metric": "cell-steps/s", "value": value, "unit": "cell-steps/s", "n_gpus": world,
+            "steps": steps_done, "warmup": args.warmup, "ms_per_step": elapsed_ms / max(steps_done, 1),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (seeded diamond-square topography, hyetograph and lognormal Ks; no dataset)",
+            "config": {"workload": f"fractal {args.nx}x{args.ny} dx=2 S=7 plain FP64 (roofline domain), "
+                                   f"steps {args.warmup}..{args.warmup + steps_done}",
+                       "cells": cells, "sclass": S, "l2": "inputs larger than L2 (state 6.7 GB), no flush",
+                       "parallelism": f"replicas x{world}", "impl": "swehr_b200 FP64, 2 kernels/step, CUDA graphs off "
+                                                                  "(per-launch event timing)"},
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": (achieved / peak) if achieved else None, "traffic": traffic,
+                         "peak_kind": peak_kind, "kernel": "k_update (FP64)",
+                         "algo_bytes_per_cell_step": B, "update_ms_avg": upd_ms},
+            "cpu_baseline": cpu,
+            "e2e": e2e,
+            "clocks": clk,
+            "gpu_launches": int(pr.kernel_launches),
+            "impl": "swehr",
+        }
+        print(json.dumps(line))
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

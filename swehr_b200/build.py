@@ -1,0 +1,74 @@
+"""Build libswehr.so in-tree with nvcc for sm_100a.
+
+  python -m swehr_b200.build            # builds swehr_b200/libswehr.so
+  python -m swehr_b200.build --ptxas-v  # also prints registers / spills per kernel
+
+The FP64 step kernels are compiled with --fmad=false: the plain form must be
+bit-identical to the CPU restatement, so no multiply-add may be contracted
+(the math bodies in swehr_math.h use explicit fma where they want one).
+"""
+from __future__ import annotations
+
+import argparse
+import os
+import subprocess
+import sys
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+CSRC = os.path.join(HERE, "csrc")
+OUT = os.path.join(HERE, "libswehr.so")
+BUILD = os.path.join(HERE, "_build")
+
+ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
+COMMON = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-I", CSRC, "-I", os.path.join(HERE, "..", "include")]
+
+# (source, extra flags)
+SOURCES = [
+    ("swehr_step_f64.cu", ["--fmad=false"]),
+    ("swehr_capi.cu", []),
+]
+
+
+def nvcc() -> str:
+    cand = os.path.join(os.environ.get("CUDA_HOME", "/usr/local/cuda"), "bin", "nvcc")
+    return cand if os.path.exists(cand) else "nvcc"
+
+
+def build(verbose: bool = False, ptxas_v: bool = False) -> str:
+    os.makedirs(BUILD, exist_ok=True)
+    objs = []
+    for src, extra in SOURCES:
+        obj = os.path.join(BUILD, os.path.splitext(src)[0] + ".o")
+        srcp = os.path.join(CSRC, src)
+        deps = [srcp] + [os.path.join(CSRC, f) for f in os.listdir(CSRC) if f.endswith((".h", ".cuh"))]
+        deps.append(os.path.join(HERE, "..", "include", "swehr.h"))
+        if not os.path.exists(obj) or any(os.path.getmtime(d) > os.path.getmtime(obj) for d in deps) or ptxas_v:
+            cmd = [nvcc()] + ARCH + COMMON + extra + ["-dc" if False else "-c", srcp, "-o", obj]
+            if ptxas_v:
+                cmd += ["-Xptxas", "-v"]
+            if verbose:
+                print(" ".join(cmd))
+            r = subprocess.run(cmd, capture_output=True, text=True)
+            if r.returncode != 0:
+                sys.stderr.write(r.stdout + r.stderr)
+                raise RuntimeError(f"nvcc failed on {src}")
+            if ptxas_v:
+                sys.stdout.write(r.stderr)
+        objs.append(obj)
+    cmd = [nvcc()] + ARCH + ["-shared", "-o", OUT] + objs + ["-lcudart"]
+    if verbose:
+        print(" ".join(cmd))
+    subprocess.check_call(cmd)
+    return OUT
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("-v", "--verbose", action="store_true")
+    ap.add_argument("--ptxas-v", action="store_true")
+    a = ap.parse_args()
+    print(build(a.verbose, a.ptxas_v))
+
+
+if __name__ == "__main__":
+    main()

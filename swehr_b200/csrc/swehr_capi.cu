@@ -1,0 +1,589 @@
+/*
+ * swehr_capi.cu -- host implementation of the C ABI in include/swehr.h.
+ *
+ * One context = one simulation on one device with its own stream.  All
+ * device memory of a context is one allocation (state sets, topography
+ * planes, Ks, rain, control block, reduction partials, stage rows), sized by
+ * swehr_footprint_bytes().  Stepping is enqueued as CUDA graphs of whole
+ * steps; the device decides when to stop (t >= tend, t_stop, step limit,
+ * CFL error), so a bounded advance is one host synchronisation at the end.
+ */
+#include <cuda_runtime.h>
+
+#include <chrono>
+#include <cmath>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/swehr.h"
+#include "swehr_kernels.h"
+
+using namespace swehr;
+
+static thread_local std::string g_last_error;
+
+static int set_err(int code, const std::string &msg)
+{
+    g_last_error = msg;
+    return code;
+}
+
+#define CK(call)                                                                                      \
+    do {                                                                                              \
+        cudaError_t e_ = (call);                                                                      \
+        if (e_ != cudaSuccess)                                                                        \
+            return set_err(SWEHR_CUDA_ERROR, std::string(#call) + ": " + cudaGetErrorString(e_));     \
+    } while (0)
+
+static const int GRAPH_STEPS = 32;
+static const int TIMING_RING = 64;
+
+struct swehr_ctx {
+    swehr_params p;
+    int precision = SWEHR_FP64;
+    int device = 0, num_sms = 148;
+    DevParams P;
+    Bufs B;
+    char *pool = nullptr;
+    size_t pool_bytes = 0;
+    double *d_rain = nullptr, *d_partials = nullptr, *d_stage = nullptr, *d_saveflow = nullptr;
+    Ctl *d_ctl = nullptr;
+    Ctl *h_ctl = nullptr;   /* pinned mirror */
+    cudaStream_t stream = nullptr;
+    cudaGraphExec_t graph = nullptr;
+    cudaEvent_t ev_start = nullptr, ev_stop = nullptr;
+    cudaEvent_t ev_k[2 * TIMING_RING] = {};
+    int grid = 1;
+    int timing = 0;
+    int64_t stagecap = 0;
+    double water_init = 0;
+    double sed_init[SWEHR_MAX_CLASSES] = {};
+};
+
+extern "C" {
+
+void swehr_params_default(swehr_params *p)
+{
+    if (!p) return;
+    memset(p, 0, sizeof *p);
+    /* SWEHR.c:490-494 */
+    p->hcfriction = 0.003; p->depthdependentexponent = -0.33; p->b = 1; p->af = 1; p->afr = 1;
+    /* SWEHR.c:632-633 */
+    p->cstable = 0.05; p->maxstep = 0.25;
+    /* SWEHR.c:638-650 */
+    p->g = 9.81; p->hfilm = 1e-5; p->phi = 0.4; p->rhos = 2600; p->rhow = 1000; p->nu = 1.2e-6;
+    p->frictionangle = 0.8693; p->cohesion = 400; p->lambda = 0.65; p->cthreshold = 0.4; p->betabedload = 0.5;
+    /* SWEHR.c:236-246 */
+    p->roughness = 0.1; p->ks = 0; p->theta0 = 0.05; p->thetas = 0.4; p->hf = 0.001; p->vinf0 = 1e-4;
+    p->uc = 0; p->uc2 = 0;
+    /* SWEHR.c:617-621 */
+    p->bndry[0] = 1; p->bndry[1] = 0; p->bndry[2] = 1; p->bndry[3] = 1;
+    p->inflow = 1;
+    /* SWEHR.c:629, 685, 709-715 */
+    p->stageint = 1; p->outlet_row = 1; p->npoints = 6;
+    const int yp[6] = {1, 10, 20, 30, 40, 50};
+    for (int m = 0; m < 6; m++) { p->xpoint[m] = 2; p->ypoint[m] = yp[m]; }
+    p->storm_radius = 1;
+}
+
+size_t swehr_params_size(void) { return sizeof(swehr_params); }
+int swehr_abi_version(void) { return SWEHR_ABI_VERSION; }
+
+const char *swehr_status_str(int s)
+{
+    switch (s) {
+    case SWEHR_OK: return "ok";
+    case SWEHR_CFL_ERROR: return "CFL error: Courant number > 1";
+    case SWEHR_NAN: return "non-finite water depth";
+    case SWEHR_TIMEOUT: return "host time limit reached";
+    case SWEHR_CUDA_ERROR: return "CUDA error";
+    case SWEHR_INVALID: return "invalid argument";
+    case SWEHR_OOM: return "out of device memory";
+    case SWEHR_NO_DEVICE: return "no CUDA device";
+    case SWEHR_BUSY: return "busy";
+    default: return "unknown status";
+    }
+}
+
+const char *swehr_last_error(void) { return g_last_error.c_str(); }
+
+}  // extern "C"
+
+static int64_t round_up(int64_t x, int64_t m) { return (x + m - 1) / m * m; }
+
+struct Layout {
+    int64_t pitch, plane, np, nplanes;
+    size_t bytes_state, off_z, off_ks, off_rain, off_ctl, off_partials, off_stage, off_saveflow, total;
+};
+
+static Layout layout_for(int nx, int ny, int S, int rnum, int has_ks, int64_t stagecap, int grid)
+{
+    Layout L;
+    L.pitch = round_up(ny, 32);
+    L.plane = round_up((int64_t)nx * L.pitch, 32);
+    L.np = P_FIXED + 2 * S;
+    L.nplanes = 2 * L.np + 3 + (has_ks ? 1 : 0);
+    size_t pb = (size_t)L.plane * sizeof(double);
+    L.bytes_state = 2 * L.np * pb;
+    L.off_z = L.bytes_state;
+    L.off_ks = L.off_z + 3 * pb;
+    L.off_rain = L.off_ks + (has_ks ? pb : 0);
+    L.off_ctl = (size_t)round_up((int64_t)(L.off_rain + (size_t)rnum * sizeof(double)), 256);
+    L.off_partials = (size_t)round_up((int64_t)(L.off_ctl + sizeof(Ctl)), 256);
+    L.off_stage = (size_t)round_up((int64_t)(L.off_partials + (size_t)grid * B_NTERMS * sizeof(double)), 256);
+    L.off_saveflow = L.off_stage + (size_t)stagecap * 24 * sizeof(double);
+    L.total = (size_t)round_up((int64_t)(L.off_saveflow + (size_t)stagecap * 18 * sizeof(double)), 256);
+    return L;
+}
+
+static int64_t stagecap_for(const swehr_params *p)
+{
+    double rows = p->stageint > 0 ? p->tend / p->stageint + 4 : 4;
+    if (!(rows < 100000)) rows = 100000;
+    return (int64_t)rows;
+}
+
+extern "C" size_t swehr_footprint_bytes(int nx, int ny, int sclass, int precision)
+{
+    (void)precision;
+    return layout_for(nx, ny, sclass, 64, 1, 4096, 148 * 4).total;
+}
+
+static int validate(const swehr_params *p, const swehr_inputs *in)
+{
+    if (!p || !in) return set_err(SWEHR_INVALID, "NULL params or inputs");
+    if (p->nx < 2 || p->ny < 2) return set_err(SWEHR_INVALID, "nx and ny must be >= 2");
+    if (p->sclass < 1 || p->sclass > SWEHR_MAX_CLASSES) return set_err(SWEHR_INVALID, "sclass must be 1..16");
+    if (p->rnum < 1) return set_err(SWEHR_INVALID, "rnum must be >= 1");
+    if (!(p->dx > 0)) return set_err(SWEHR_INVALID, "dx must be > 0");
+    if (!(p->rint > 0) && !(p->storm_peak > 0)) return set_err(SWEHR_INVALID, "rint must be > 0");
+    for (int k = 0; k < 4; k++)
+        if (p->bndry[k] != 0 && p->bndry[k] != 1) return set_err(SWEHR_INVALID, "bndry values must be 0 or 1");
+    if (p->outlet_row < 1 || p->outlet_row > p->ny) return set_err(SWEHR_INVALID, "outlet_row outside 1..ny");
+    if (p->storm_peak > 0 && !(p->storm_radius > 0)) return set_err(SWEHR_INVALID, "storm_radius must be > 0");
+    if (!in->topo || !in->rain || !in->ds || !in->pfrac) return set_err(SWEHR_INVALID, "NULL input array");
+    return SWEHR_OK;
+}
+
+static void make_devparams(const swehr_params *p, const swehr_inputs *in, const Layout &L, DevParams &P)
+{
+    memset(&P, 0, sizeof P);
+    P.nx = p->nx; P.ny = p->ny; P.S = p->sclass; P.pitch = (int32_t)L.pitch;
+    P.rnum = p->rnum; P.inflow = p->inflow ? 1 : 0; P.storm = p->storm_peak > 0; P.budget = p->budget ? 1 : 0;
+    for (int k = 0; k < 4; k++) P.bndry[k] = p->bndry[k];
+    P.outlet_row = p->outlet_row; P.npoints = p->npoints;
+    for (int m = 0; m < 6; m++) { P.xpoint[m] = p->xpoint[m]; P.ypoint[m] = p->ypoint[m]; }
+    P.has_ks = in->ks != nullptr;
+    P.plane = L.plane;
+    P.dx = p->dx; P.oneoverdx = 1 / p->dx; P.half_odx = 0.5 * P.oneoverdx; P.tend = p->tend; P.rint = p->rint;
+    P.stageint = p->stageint;
+    P.g = p->g; P.hfilm = p->hfilm; P.hfx10 = 10 * p->hfilm; P.rhos = p->rhos; P.rhow = p->rhow;
+    P.rho0 = p->rhow * p->phi + p->rhos * (1 - p->phi);
+    P.porod = p->rhos * (1 - p->phi);
+    P.invporo = 1 / (p->rhos * (1 - p->phi));
+    P.nu = p->nu; P.fa = p->frictionangle; P.cohesion = p->cohesion; P.neg1ml = -(1 - p->lambda);
+    P.cthreshold = p->cthreshold; P.one_m_bb = 1 - p->betabedload; P.hc = p->hcfriction;
+    P.dde = p->depthdependentexponent; P.b = p->b; P.af = p->af; P.afr = p->afr;
+    P.h0 = p->h0; P.h0x3 = 3 * p->h0; P.h0x6 = 6 * p->h0; P.h0x9 = 9 * p->h0; P.mtstar0 = p->mtstar0;
+    P.a = p->a; P.ad = p->ad; P.F = p->F; P.J = p->J;
+    P.roughness = p->roughness; P.ks = p->ks; P.theta0 = p->theta0; P.thetas = p->thetas; P.hf = p->hf;
+    P.uc = p->uc; P.uc2 = p->uc2; P.cstable = p->cstable; P.maxstep = p->maxstep;
+    P.c109s = 1.09 * (p->rhos / p->rhow - 1);
+    P.rhos08 = 0.8 * p->rhos;
+    P.storm_peak = p->storm_peak; P.storm_r2 = p->storm_radius * p->storm_radius;
+    P.storm_x0 = p->storm_x0; P.storm_y0 = p->storm_y0; P.storm_vx = p->storm_vx; P.storm_vy = p->storm_vy;
+    for (int k = 0; k < p->sclass; k++) {
+        P.ds[k] = in->ds[k];
+        P.pf[k] = in->pfrac[k];
+        P.a13[k] = 13.95 * p->nu / in->ds[k];
+        P.a13sq[k] = P.a13[k] * P.a13[k];
+    }
+}
+
+static int upload_plane(swehr_ctx *c, double *dplane, const double *host, cudaStream_t s)
+{
+    CK(cudaMemcpy2DAsync(dplane, (size_t)c->P.pitch * sizeof(double), host, (size_t)c->P.ny * sizeof(double),
+                         (size_t)c->P.ny * sizeof(double), (size_t)c->P.nx, cudaMemcpyHostToDevice, s));
+    return SWEHR_OK;
+}
+
+static int download_plane(swehr_ctx *c, double *host, const double *dplane, cudaStream_t s)
+{
+    CK(cudaMemcpy2DAsync(host, (size_t)c->P.ny * sizeof(double), dplane, (size_t)c->P.pitch * sizeof(double),
+                         (size_t)c->P.ny * sizeof(double), (size_t)c->P.nx, cudaMemcpyDeviceToHost, s));
+    return SWEHR_OK;
+}
+
+static void destroy_ctx(swehr_ctx *c)
+{
+    if (!c) return;
+    if (c->stream) cudaStreamSynchronize(c->stream);
+    if (c->graph) cudaGraphExecDestroy(c->graph);
+    if (c->ev_start) cudaEventDestroy(c->ev_start);
+    if (c->ev_stop) cudaEventDestroy(c->ev_stop);
+    for (int e = 0; e < 2 * TIMING_RING; e++)
+        if (c->ev_k[e]) cudaEventDestroy(c->ev_k[e]);
+    if (c->pool) cudaFree(c->pool);
+    if (c->h_ctl) cudaFreeHost(c->h_ctl);
+    if (c->stream) cudaStreamDestroy(c->stream);
+    delete c;
+}
+
+extern "C" int swehr_create(const swehr_params *p, const swehr_inputs *in, int precision, swehr_ctx **out)
+{
+    if (!out) return set_err(SWEHR_INVALID, "NULL out");
+    *out = nullptr;
+    int v = validate(p, in);
+    if (v) return v;
+    if (precision != SWEHR_FP64) return set_err(SWEHR_INVALID, "precision not supported by this build");
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev < 1) return set_err(SWEHR_NO_DEVICE, "no CUDA device");
+    swehr_ctx *c = new swehr_ctx();
+    c->p = *p;
+    c->precision = precision;
+    int rc;
+#define CKC(call)                                                                               \
+    do {                                                                                        \
+        cudaError_t e_ = (call);                                                                \
+        if (e_ != cudaSuccess) {                                                                \
+            rc = set_err(e_ == cudaErrorMemoryAllocation ? SWEHR_OOM : SWEHR_CUDA_ERROR,        \
+                         std::string(#call) + ": " + cudaGetErrorString(e_));                   \
+            destroy_ctx(c);                                                                     \
+            return rc;                                                                          \
+        }                                                                                       \
+    } while (0)
+    CKC(cudaGetDevice(&c->device));
+    CKC(cudaDeviceGetAttribute(&c->num_sms, cudaDevAttrMultiProcessorCount, c->device));
+    c->stagecap = stagecap_for(p);
+    DevParams tmpP;
+    Layout L0 = layout_for(p->nx, p->ny, p->sclass, p->rnum, in->ks != nullptr, c->stagecap, 1);
+    make_devparams(p, in, L0, tmpP);
+    c->grid = step_grid_f64(tmpP, c->num_sms);
+    Layout L = layout_for(p->nx, p->ny, p->sclass, p->rnum, in->ks != nullptr, c->stagecap, c->grid);
+    make_devparams(p, in, L, c->P);
+    CKC(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
+    CKC(cudaMalloc((void **)&c->pool, L.total));
+    c->pool_bytes = L.total;
+    CKC(cudaMemsetAsync(c->pool, 0, L.total, c->stream));
+    double *base = (double *)c->pool;
+    c->B.set[0] = base;
+    c->B.set[1] = base + L.np * L.plane;
+    for (int k = 0; k < 3; k++) c->B.z[k] = (double *)(c->pool + L.off_z) + k * L.plane;
+    c->B.ks = in->ks ? (const double *)(c->pool + L.off_ks) : nullptr;
+    c->d_rain = (double *)(c->pool + L.off_rain);
+    c->d_ctl = (Ctl *)(c->pool + L.off_ctl);
+    c->d_partials = (double *)(c->pool + L.off_partials);
+    c->d_stage = (double *)(c->pool + L.off_stage);
+    c->d_saveflow = (double *)(c->pool + L.off_saveflow);
+    CKC(cudaMallocHost((void **)&c->h_ctl, sizeof(Ctl)));
+    CKC(cudaEventCreate(&c->ev_start));
+    CKC(cudaEventCreate(&c->ev_stop));
+    for (int e = 0; e < 2 * TIMING_RING; e++) CKC(cudaEventCreate(&c->ev_k[e]));
+    /* initial state (initialcondition, SWEHR.c:211-285): dry bed, VINF = vinf0, z = topo;
+     * z of the previous step = z (setup slopes, SWEHR.c:721-803) */
+    for (int k = 0; k < 3; k++) {
+        rc = upload_plane(c, c->B.z[k], in->topo, c->stream);
+        if (rc) { destroy_ctx(c); return rc; }
+    }
+    if (in->ks) {
+        rc = upload_plane(c, (double *)c->B.ks, in->ks, c->stream);
+        if (rc) { destroy_ctx(c); return rc; }
+    }
+    {
+        std::vector<double> row((size_t)c->P.plane, 0.0);
+        for (int i = 0; i < p->nx; i++)
+            for (int j = 0; j < p->ny; j++) row[(size_t)i * c->P.pitch + j] = p->vinf0;
+        CKC(cudaMemcpyAsync(c->B.set[0] + P_VINF * c->P.plane, row.data(), (size_t)c->P.plane * sizeof(double),
+                            cudaMemcpyHostToDevice, c->stream));
+        CKC(cudaMemcpyAsync(c->d_rain, in->rain, (size_t)p->rnum * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+        Ctl h;
+        memset(&h, 0, sizeof h);
+        h.t = 0;
+        h.stagecap = c->stagecap;
+        h.t_stop = INFINITY;
+        *c->h_ctl = h;
+        CKC(cudaMemcpyAsync(c->d_ctl, c->h_ctl, sizeof(Ctl), cudaMemcpyHostToDevice, c->stream));
+        CKC(cudaStreamSynchronize(c->stream));
+    }
+    c->water_init = (double)p->nx * (double)p->ny * p->vinf0;
+    *out = c;
+    return SWEHR_OK;
+#undef CKC
+}
+
+extern "C" void swehr_destroy(swehr_ctx *c) { destroy_ctx(c); }
+
+extern "C" int swehr_set_timing(swehr_ctx *c, int on)
+{
+    if (!c) return set_err(SWEHR_INVALID, "NULL ctx");
+    c->timing = on ? 1 : 0;
+    return SWEHR_OK;
+}
+
+static int build_graph(swehr_ctx *c)
+{
+    if (c->graph) return SWEHR_OK;
+    cudaGraph_t g;
+    CK(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
+    for (int s = 0; s < GRAPH_STEPS; s++)
+        launch_step_f64(c->P, c->B, c->d_ctl, c->d_rain, c->d_partials, c->d_stage, c->d_saveflow, c->grid,
+                        c->stream, nullptr, nullptr);
+    CK(cudaStreamEndCapture(c->stream, &g));
+    cudaError_t e = cudaGraphInstantiate(&c->graph, g, 0);
+    cudaGraphDestroy(g);
+    if (e != cudaSuccess) return set_err(SWEHR_CUDA_ERROR, std::string("cudaGraphInstantiate: ") + cudaGetErrorString(e));
+    return SWEHR_OK;
+}
+
+extern "C" int swehr_advance(swehr_ctx *c, double t_stop, int64_t max_steps, swehr_progress *pr)
+{
+    if (!c) return set_err(SWEHR_INVALID, "NULL ctx");
+    auto wall0 = std::chrono::steady_clock::now();
+    /* read the control block, arm it */
+    CK(cudaMemcpyAsync(c->h_ctl, c->d_ctl, sizeof(Ctl), cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    Ctl *h = c->h_ctl;
+    const int64_t step0 = h->step;
+    if (h->status == SWEHR_CFL_ERROR) {
+        if (pr) {
+            memset(pr, 0, sizeof *pr);
+            pr->t = h->t; pr->steps = h->step; pr->status = SWEHR_CFL_ERROR; pr->done = 1;
+        }
+        return SWEHR_CFL_ERROR;
+    }
+    double kernel_ms = 0;
+    int64_t launched = 0;
+    bool run = h->t < c->p.tend && h->t < t_stop && max_steps != 0;
+    if (run) {
+        h->t_stop = t_stop;
+        h->max_step = max_steps < 0 ? INT64_MAX : step0 + max_steps;
+        h->active = 1;
+        h->pending = 0;
+        CK(cudaMemcpyAsync(c->d_ctl, h, sizeof(Ctl), cudaMemcpyHostToDevice, c->stream));
+        CK(cudaEventRecord(c->ev_start, c->stream));
+        if (c->timing) {
+            int64_t left = max_steps;
+            for (;;) {
+                int n = TIMING_RING;
+                if (max_steps >= 0 && left < n) n = (int)left;
+                for (int s = 0; s < n; s++) {
+                    int e = launch_step_f64(c->P, c->B, c->d_ctl, c->d_rain, c->d_partials, c->d_stage, c->d_saveflow,
+                                            c->grid, c->stream, c->ev_k[2 * s], c->ev_k[2 * s + 1]);
+                    if (e) return set_err(SWEHR_CUDA_ERROR, std::string("launch: ") + cudaGetErrorString((cudaError_t)e));
+                }
+                launched += 2 * n;
+                CK(cudaMemcpyAsync(h, c->d_ctl, sizeof(Ctl), cudaMemcpyDeviceToHost, c->stream));
+                CK(cudaStreamSynchronize(c->stream));
+                for (int s = 0; s < n; s++) {
+                    float ms = 0;
+                    CK(cudaEventElapsedTime(&ms, c->ev_k[2 * s], c->ev_k[2 * s + 1]));
+                    kernel_ms += ms;
+                }
+                if (max_steps >= 0) left -= n;
+                if (!h->active || (max_steps >= 0 && left <= 0)) break;
+            }
+        } else {
+            int rcg = build_graph(c);
+            if (rcg) return rcg;
+            if (max_steps >= 0) {
+                int64_t full = max_steps / GRAPH_STEPS, rem = max_steps % GRAPH_STEPS;
+                for (int64_t gi = 0; gi < full; gi++) CK(cudaGraphLaunch(c->graph, c->stream));
+                for (int64_t s = 0; s < rem; s++)
+                    launch_step_f64(c->P, c->B, c->d_ctl, c->d_rain, c->d_partials, c->d_stage, c->d_saveflow,
+                                    c->grid, c->stream, nullptr, nullptr);
+                launched = 2 * max_steps;
+                CK(cudaGetLastError());
+                CK(cudaMemcpyAsync(h, c->d_ctl, sizeof(Ctl), cudaMemcpyDeviceToHost, c->stream));
+                CK(cudaStreamSynchronize(c->stream));
+            } else {
+                for (;;) {
+                    for (int gi = 0; gi < 4; gi++) CK(cudaGraphLaunch(c->graph, c->stream));
+                    launched += 2 * 4 * GRAPH_STEPS;
+                    CK(cudaMemcpyAsync(h, c->d_ctl, sizeof(Ctl), cudaMemcpyDeviceToHost, c->stream));
+                    CK(cudaStreamSynchronize(c->stream));
+                    if (!h->active) break;
+                }
+            }
+        }
+        CK(cudaEventRecord(c->ev_stop, c->stream));
+        CK(cudaStreamSynchronize(c->stream));
+    }
+    float dev_ms = 0;
+    if (run) CK(cudaEventElapsedTime(&dev_ms, c->ev_start, c->ev_stop));
+    int st = h->status;
+    (void)wall0;
+    if (pr) {
+        memset(pr, 0, sizeof *pr);
+        pr->t = h->t; pr->dt = h->dt; pr->courant = h->courant;
+        pr->rain = 0;
+        pr->steps = h->step;
+        pr->steps_this_call = h->step - step0;
+        pr->device_ms = dev_ms;
+        pr->kernel_ms = kernel_ms;
+        pr->kernel_launches = launched;
+        pr->status = st;
+        pr->done = !(h->t < c->p.tend);
+    }
+    return st;
+}
+
+static double *field_plane(swehr_ctx *c, int field, int k, int cur)
+{
+    double *set = c->B.set[cur];
+    int64_t pl = c->P.plane;
+    switch (field) {
+    case SWEHR_FIELD_H: return set + P_H * pl;
+    case SWEHR_FIELD_HU: return set + P_HU * pl;
+    case SWEHR_FIELD_HV: return set + P_HV * pl;
+    case SWEHR_FIELD_VINF: return set + P_VINF * pl;
+    case SWEHR_FIELD_MAXVEL: return set + P_MAXVEL * pl;
+    case SWEHR_FIELD_MAXDEPTH: return set + P_MAXDEP * pl;
+    case SWEHR_FIELD_TOTM: return set + P_TOTM * pl;
+    case SWEHR_FIELD_DEP: return set + P_DEP * pl;
+    case SWEHR_FIELD_TOTSED: return set + P_TOTSED * pl;
+    case SWEHR_FIELD_U: return set + (P_FIXED + k - 1) * pl;
+    case SWEHR_FIELD_M: return set + (P_FIXED + c->P.S + k - 1) * pl;
+    default: return nullptr;
+    }
+}
+
+static int current_step(swehr_ctx *c, int64_t *step)
+{
+    CK(cudaMemcpyAsync(c->h_ctl, c->d_ctl, sizeof(Ctl), cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    *step = c->h_ctl->step;
+    return SWEHR_OK;
+}
+
+extern "C" int swehr_read_field(swehr_ctx *c, int field, int k, double *dst)
+{
+    if (!c || !dst) return set_err(SWEHR_INVALID, "NULL argument");
+    const int S = c->P.S;
+    if ((field == SWEHR_FIELD_U || field == SWEHR_FIELD_M || field == SWEHR_FIELD_SED) && (k < 1 || k > S))
+        return set_err(SWEHR_INVALID, "class index out of range");
+    int64_t step;
+    int rc = current_step(c, &step);
+    if (rc) return rc;
+    const int cur = (int)(step & 1);
+    const size_t N = (size_t)c->P.nx * c->P.ny;
+    const double hfilm = c->P.hfilm;
+    if (field == SWEHR_FIELD_Z) {
+        rc = download_plane(c, dst, c->B.z[step % 3], c->stream);
+    } else if (field == SWEHR_FIELD_VEL || field == SWEHR_FIELD_SED) {
+        std::vector<double> h(N), a(N), b(N);
+        rc = download_plane(c, h.data(), field_plane(c, SWEHR_FIELD_H, 0, cur), c->stream);
+        if (!rc) rc = download_plane(c, a.data(), field_plane(c, field == SWEHR_FIELD_VEL ? SWEHR_FIELD_HU : SWEHR_FIELD_U, k, cur), c->stream);
+        if (!rc && field == SWEHR_FIELD_VEL) rc = download_plane(c, b.data(), field_plane(c, SWEHR_FIELD_HV, 0, cur), c->stream);
+        if (rc) return rc;
+        CK(cudaStreamSynchronize(c->stream));
+        for (size_t q = 0; q < N; q++) {
+            if (field == SWEHR_FIELD_VEL) {
+                double v1 = h[q] > hfilm ? a[q] / h[q] : 0, v2 = h[q] > hfilm ? b[q] / h[q] : 0;
+                double s = std::sqrt(v1 * v1 + v2 * v2);
+                dst[q] = (s == 0.0) ? 0.0 : s;
+            } else {
+                double s = h[q] > hfilm ? a[q] / h[q] : 0.0;
+                dst[q] = (h[q] > hfilm && s < -1e-5) ? 0.0 : s;
+            }
+        }
+        return SWEHR_OK;
+    } else {
+        double *src = field_plane(c, field, k, cur);
+        if (!src) return set_err(SWEHR_INVALID, "unknown field");
+        rc = download_plane(c, dst, src, c->stream);
+    }
+    if (rc) return rc;
+    CK(cudaStreamSynchronize(c->stream));
+    return SWEHR_OK;
+}
+
+extern "C" int swehr_write_field(swehr_ctx *c, int field, int k, const double *src)
+{
+    if (!c || !src) return set_err(SWEHR_INVALID, "NULL argument");
+    int64_t step;
+    int rc = current_step(c, &step);
+    if (rc) return rc;
+    const int cur = (int)(step & 1);
+    if (field == SWEHR_FIELD_Z) {
+        rc = upload_plane(c, c->B.z[step % 3], src, c->stream);
+        if (!rc) rc = upload_plane(c, c->B.z[(step + 2) % 3], src, c->stream);
+    } else {
+        if ((field == SWEHR_FIELD_U || field == SWEHR_FIELD_M) && (k < 1 || k > c->P.S))
+            return set_err(SWEHR_INVALID, "class index out of range");
+        if (field == SWEHR_FIELD_VEL || field == SWEHR_FIELD_SED) return set_err(SWEHR_INVALID, "derived field");
+        double *dstp = field_plane(c, field, k, cur);
+        if (!dstp) return set_err(SWEHR_INVALID, "unknown field");
+        rc = upload_plane(c, dstp, src, c->stream);
+    }
+    if (rc) return rc;
+    CK(cudaStreamSynchronize(c->stream));
+    return SWEHR_OK;
+}
+
+extern "C" int swehr_read_series(swehr_ctx *c, double *stage, double *saveflow, int64_t max_rows, int64_t *rows)
+{
+    if (!c) return set_err(SWEHR_INVALID, "NULL ctx");
+    int64_t step;
+    int rc = current_step(c, &step);
+    if (rc) return rc;
+    int64_t n = c->h_ctl->stagecnt < max_rows ? c->h_ctl->stagecnt : max_rows;
+    if (n > 0 && stage) CK(cudaMemcpyAsync(stage, c->d_stage, (size_t)n * 24 * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    if (n > 0 && saveflow)
+        CK(cudaMemcpyAsync(saveflow, c->d_saveflow, (size_t)n * 18 * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    if (rows) *rows = n;
+    return SWEHR_OK;
+}
+
+/* compensated (Neumaier) sum of a field over the interior */
+static double sum_plane(const std::vector<double> &a)
+{
+    double s = 0, comp = 0;
+    for (double v : a) {
+        double t = s + v;
+        if (std::fabs(s) >= std::fabs(v)) comp += (s - t) + v;
+        else comp += (v - t) + s;
+        s = t;
+    }
+    return s + comp;
+}
+
+extern "C" int swehr_get_budget(swehr_ctx *c, swehr_budget *b)
+{
+    if (!c || !b) return set_err(SWEHR_INVALID, "NULL argument");
+    memset(b, 0, sizeof *b);
+    const size_t N = (size_t)c->P.nx * c->P.ny;
+    std::vector<double> h(N), vi(N), tmp(N), tmp2(N);
+    int rc = swehr_read_field(c, SWEHR_FIELD_H, 0, h.data());
+    if (!rc) rc = swehr_read_field(c, SWEHR_FIELD_VINF, 0, vi.data());
+    if (rc) return rc;
+    for (size_t q = 0; q < N; q++) tmp[q] = h[q];
+    double wsum = sum_plane(tmp) + sum_plane(vi);
+    const Ctl *H = c->h_ctl;
+    auto term = [&](int m) { return H->budget_hi[m] + H->budget_lo[m]; };
+    b->water_now = wsum;
+    b->water_init = c->water_init;
+    b->rain_in = term(B_RAIN);
+    b->outflow = term(B_OUT);
+    b->clamp_gain = term(B_CLAMP);
+    b->bulking = term(B_BULK);
+    b->infiltration = term(B_INF);
+    b->water_residual = (wsum - c->water_init) - (b->rain_in - b->outflow + b->clamp_gain + b->bulking);
+    b->sclass = c->P.S;
+    for (int k = 0; k < c->P.S; k++) {
+        rc = swehr_read_field(c, SWEHR_FIELD_U, k + 1, tmp.data());
+        if (!rc) rc = swehr_read_field(c, SWEHR_FIELD_M, k + 1, tmp2.data());
+        if (rc) return rc;
+        double s = sum_plane(tmp) + sum_plane(tmp2);
+        b->sed_now[k] = s;
+        b->sed_init[k] = c->sed_init[k];
+        b->detach[k] = term(B_DET + k);
+        b->sed_outflow[k] = term(B_SOUT + k);
+        b->sed_residual[k] = (s - c->sed_init[k]) - (b->detach[k] - b->sed_outflow[k]);
+    }
+    b->valid = c->P.budget;
+    return SWEHR_OK;
+}

@@ -1,0 +1,23 @@
+/* swehr_kernels.h -- host-visible launch entry points of the step kernels. */
+#pragma once
+#include <cuda_runtime.h>
+
+#include "swehr_device.cuh"
+
+namespace swehr {
+
+/* device buffers of one simulation: two state sets (9 + 2S planes each),
+ * three topography planes, optional per-cell Ks */
+struct Bufs {
+    double *set[2];
+    double *z[3];
+    const double *ks;
+};
+
+/* Enqueue one full step (wave pass + update pass) of the FP64 form.
+ * ev0/ev1 (optional) are recorded around the update kernel. */
+int launch_step_f64(const DevParams &P, const Bufs &B, Ctl *ctl, const double *rain, double *partials,
+                    double *stage, double *saveflow, int grid, cudaStream_t s, cudaEvent_t ev0, cudaEvent_t ev1);
+int step_grid_f64(const DevParams &P, int num_sms);
+
+}  // namespace swehr

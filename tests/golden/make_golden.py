@@ -1,0 +1,101 @@
+"""Generate the golden fixtures in tests/golden/ from the reference program.
+
+The reference (SWEHR.c) ships no tests, golden vectors or known answers;
+its only example is the 3x51 strip in input.txt/topoin.txt.  The fixtures
+here are outputs of the reference itself, built from its source by
+oracle/build_ref.py, on:
+
+  shipped.npz       the shipped example's input files and the reference's
+                    state after 2000 and 20000 steps (inflow on, default BCs;
+                    the last row of M is NaN, a reference 0/0 at t=0)
+  tiny_*.npz        small random hillslopes, every boundary type, inflow
+                    on and off, per-cell Ks, to the end of their event
+  hillslope.npz     the 200x50 hillslope, full 1200 s run, and the state at
+                    600 s (mid-event, wet)
+
+Each file holds the Case (params as JSON, topo, rain, ds, pfrac, ks) and the
+reference's %.17g dump of every state field.
+
+Run (needs the reference checkout; it is not read anywhere else):
+    python tests/golden/make_golden.py [--reference /root/reference]
+"""
+import argparse
+import json
+import os
+import sys
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(os.path.dirname(HERE))
+sys.path.insert(0, ROOT)
+sys.path.insert(0, os.path.join(ROOT, "tests"))
+
+from swehr_b200 import io as swio, workloads as W  # noqa: E402
+from swehr_b200.params import REFERENCE_DEFAULTS  # noqa: E402
+import harness  # noqa: E402
+
+TINY = [
+    dict(nx=12, ny=9, S=3, seed=5, bndry=(0, 1, 1, 1), inflow=0, rain_mmh=90.0, tend=60.0),
+    dict(nx=15, ny=11, S=4, seed=6, bndry=(1, 0, 1, 1), inflow=1, rain_mmh=300.0, tend=120.0),
+    dict(nx=15, ny=11, S=4, seed=7, bndry=(0, 0, 0, 0), inflow=0, rain_mmh=300.0, tend=120.0),
+    dict(nx=9, ny=14, S=2, seed=8, bndry=(1, 1, 1, 1), inflow=1, rain_mmh=200.0, tend=90.0, per_cell_ks=False),
+    dict(nx=20, ny=6, S=7, seed=9, bndry=(0, 1, 0, 1), inflow=0, rain_mmh=500.0, tend=150.0),
+]
+
+DUMP_KEYS = ("h", "hu", "hv", "z", "vinf", "totm", "dep", "totsed", "maxvel", "maxdepth", "U", "M", "sed",
+             "stage", "saveflow")
+
+
+def save(path, case, dumps: dict):
+    arrs = {"params_json": np.array(json.dumps(case.params)), "topo": case.topo, "rain": case.rain,
+            "ds": case.ds, "pfrac": case.pfrac, "name": np.array(case.name)}
+    if case.ks is not None:
+        arrs["ks"] = case.ks
+    for tag, d in dumps.items():
+        arrs[f"{tag}__steps"] = np.array(d["steps"])
+        arrs[f"{tag}__t"] = np.array(d["t"])
+        for k in DUMP_KEYS:
+            arrs[f"{tag}__{k}"] = d[k]
+    np.savez_compressed(path, **arrs)
+    print("wrote", path, os.path.getsize(path), "bytes")
+
+
+def shipped_case(reference):
+    c = swio.read_inputs(reference)
+    for k in ("bndry", "inflow", "roughness", "ks", "theta0", "thetas", "hf", "vinf0", "uc", "uc2"):
+        c.params[k] = REFERENCE_DEFAULTS[k]
+    c.params["bndry"] = list(c.params["bndry"])
+    c.name = "shipped"
+    return c
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--reference", default="/root/reference")
+    a = ap.parse_args()
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import build_ref
+    if not build_ref.build(a.reference):
+        raise SystemExit("reference not available")
+    c = shipped_case(a.reference)
+    d1, _ = harness.run_reference(c, max_steps=2000)
+    d2, _ = harness.run_reference(c, max_steps=20000)
+    save(os.path.join(HERE, "shipped.npz"), c, {"s2000": d1, "s20000": d2})
+    for n, kw in enumerate(TINY):
+        c = W.tiny_case(**kw)
+        c.params["bndry"] = list(c.params["bndry"])
+        d, _ = harness.run_reference(c)
+        save(os.path.join(HERE, f"tiny_{n}.npz"), c, {"end": d})
+    c = W.hillslope200x50()
+    c.params["bndry"] = list(c.params["bndry"])
+    c600 = W.hillslope200x50()
+    c600.params["bndry"] = list(c600.params["bndry"])
+    c600.params["tend"] = 600.0
+    dmid, _ = harness.run_reference(c600)
+    dend, _ = harness.run_reference(c)
+    save(os.path.join(HERE, "hillslope.npz"), c, {"t600": dmid, "end": dend})
+
+
+if __name__ == "__main__":
+    main()

@@ -187,3 +187,27 @@ def compare(a: dict, b: dict, names=STATE_FIELDS + CLASS_FIELDS) -> dict:
         bit = same_nan and bool(np.array_equal(x[m], y[m]))
         out[n] = (float(rel), same_nan, bit)
     return out
+
+
+GOLDEN_DIR = os.path.join(ROOT, "tests", "golden")
+
+
+def load_golden(name: str):
+    """(Case, {tag: {field: array}}) from tests/golden/<name>.npz."""
+    import json
+    from swehr_b200.workloads import Case
+    z = np.load(os.path.join(GOLDEN_DIR, name + ".npz"), allow_pickle=False)
+    params = json.loads(str(z["params_json"]))
+    if "bndry" in params:
+        params["bndry"] = tuple(params["bndry"])
+    case = Case(str(z["name"]), params, z["topo"], z["rain"], z["ds"], z["pfrac"],
+                ks=z["ks"] if "ks" in z.files else None)
+    dumps = {}
+    for key in z.files:
+        if "__" in key:
+            tag, f = key.split("__", 1)
+            dumps.setdefault(tag, {})[f] = z[key]
+    for d in dumps.values():
+        d["steps"] = int(d["steps"])
+        d["t"] = float(d["t"])
+    return case, dumps
