@@ -190,6 +190,26 @@ size_t swehr_footprint_bytes(int nx, int ny, int sclass, int precision);
 
 void swehr_destroy(swehr_ctx *ctx);
 
+/* No counterpart in the reference (SWEHR.c computes dt on the host inside
+ * main, SWEHR.c:1409-1411, and has no device).  The CFL time step of one
+ * state, for callers that cannot allocate device memory -- a framework that
+ * owns every allocation through its own pool, or code running where the
+ * allocator is locked: nothing is allocated; the kernel's scratch is a fixed
+ * file-scope device array of 128.25 KiB held by every GPU that loads the
+ * library.  d_h, d_hu, d_hv, d_zprev are caller-owned device planes of nx rows
+ * by `pitch` doubles (cell (i,j) at [(i-1)*pitch + (j-1)]; d_zprev is the
+ * topography of the previous step, or the current one at the first step);
+ * d_result (device, 2 doubles) receives {Smax, dt} exactly as the update
+ * path's wave pass computes them.  Asynchronous on `stream` (a cudaStream_t,
+ * NULL for the legacy default stream).  Domains above SWEHR_NOALLOC_MAX_CELLS
+ * cells are rejected with SWEHR_INVALID.  The first call on a device looks up
+ * the scratch address there (make it before any stream capture); calls that
+ * overlap on the GPU share the scratch and race -- serialise them. */
+#define SWEHR_NOALLOC_MAX_CELLS 16777216
+#define SWEHR_NOALLOC_MAX_BLOCKS 16384
+int swehr_cfl_noalloc(const swehr_params *p, const double *d_h, const double *d_hu, const double *d_hv,
+                      const double *d_zprev, int64_t pitch, double t, double *d_result, void *stream);
+
 #ifdef __cplusplus
 }
 #endif

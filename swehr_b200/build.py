@@ -26,6 +26,7 @@ COMMON = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-I", CSRC, "
 SOURCES = [
     ("swehr_step_f64.cu", ["--fmad=false"]),
     ("swehr_capi.cu", []),
+    ("swehr_cfl_noalloc.cu", ["--fmad=false"]),
 ]
 
 

@@ -110,6 +110,9 @@ const char *swehr_status_str(int s)
 
 const char *swehr_last_error(void) { return g_last_error.c_str(); }
 
+/* lets other translation units of the library report an error message */
+void swehr_set_last_error(const char *msg) { g_last_error = msg ? msg : ""; }
+
 }  // extern "C"
 
 static int64_t round_up(int64_t x, int64_t m) { return (x + m - 1) / m * m; }

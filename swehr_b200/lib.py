@@ -56,6 +56,8 @@ def load() -> C.CDLL:
     L.swehr_footprint_bytes.restype = C.c_size_t
     L.swehr_footprint_bytes.argtypes = [i32, i32, i32, i32]
     L.swehr_destroy.argtypes = [vp]
+    L.swehr_cfl_noalloc.restype = i32
+    L.swehr_cfl_noalloc.argtypes = [vp, vp, vp, vp, vp, i64, dbl, vp, vp]
     if L.swehr_params_size() != C.sizeof(SwehrParams):
         raise ImportError(f"swehr_params size mismatch: C {L.swehr_params_size()} vs ctypes {C.sizeof(SwehrParams)}")
     _lib = L
