@@ -56,7 +56,7 @@ struct swehr_ctx {
     cudaGraphExec_t graph = nullptr;
     cudaEvent_t ev_start = nullptr, ev_stop = nullptr;
     cudaEvent_t ev_k[2 * TIMING_RING] = {};
-    int grid = 1;
+    StepConfig cfg;
     int timing = 0;
     int64_t stagecap = 0;
     double water_init = 0;
@@ -264,8 +264,15 @@ extern "C" int swehr_create(const swehr_params *p, const swehr_inputs *in, int p
     DevParams tmpP;
     Layout L0 = layout_for(p->nx, p->ny, p->sclass, p->rnum, in->ks != nullptr, c->stagecap, 1);
     make_devparams(p, in, L0, tmpP);
-    c->grid = step_grid_f64(tmpP, c->num_sms);
-    Layout L = layout_for(p->nx, p->ny, p->sclass, p->rnum, in->ks != nullptr, c->stagecap, c->grid);
+    {
+        int ce = configure_step_f64(tmpP, c->num_sms, c->cfg);
+        if (ce) {
+            rc = set_err(SWEHR_CUDA_ERROR, std::string("configure: ") + cudaGetErrorString((cudaError_t)ce));
+            destroy_ctx(c);
+            return rc;
+        }
+    }
+    Layout L = layout_for(p->nx, p->ny, p->sclass, p->rnum, in->ks != nullptr, c->stagecap, c->cfg.grid_update);
     make_devparams(p, in, L, c->P);
     CKC(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
     CKC(cudaMalloc((void **)&c->pool, L.total));
@@ -332,7 +339,7 @@ static int build_graph(swehr_ctx *c)
     cudaGraph_t g;
     CK(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
     for (int s = 0; s < GRAPH_STEPS; s++)
-        launch_step_f64(c->P, c->B, c->d_ctl, c->d_rain, c->d_partials, c->d_stage, c->d_saveflow, c->grid,
+        launch_step_f64(c->P, c->B, c->d_ctl, c->d_rain, c->d_partials, c->d_stage, c->d_saveflow, c->cfg,
                         c->stream, nullptr, nullptr);
     CK(cudaStreamEndCapture(c->stream, &g));
     cudaError_t e = cudaGraphInstantiate(&c->graph, g, 0);
@@ -374,7 +381,7 @@ extern "C" int swehr_advance(swehr_ctx *c, double t_stop, int64_t max_steps, swe
                 if (max_steps >= 0 && left < n) n = (int)left;
                 for (int s = 0; s < n; s++) {
                     int e = launch_step_f64(c->P, c->B, c->d_ctl, c->d_rain, c->d_partials, c->d_stage, c->d_saveflow,
-                                            c->grid, c->stream, c->ev_k[2 * s], c->ev_k[2 * s + 1]);
+                                            c->cfg, c->stream, c->ev_k[2 * s], c->ev_k[2 * s + 1]);
                     if (e) return set_err(SWEHR_CUDA_ERROR, std::string("launch: ") + cudaGetErrorString((cudaError_t)e));
                 }
                 launched += 2 * n;
@@ -396,7 +403,7 @@ extern "C" int swehr_advance(swehr_ctx *c, double t_stop, int64_t max_steps, swe
                 for (int64_t gi = 0; gi < full; gi++) CK(cudaGraphLaunch(c->graph, c->stream));
                 for (int64_t s = 0; s < rem; s++)
                     launch_step_f64(c->P, c->B, c->d_ctl, c->d_rain, c->d_partials, c->d_stage, c->d_saveflow,
-                                    c->grid, c->stream, nullptr, nullptr);
+                                    c->cfg, c->stream, nullptr, nullptr);
                 launched = 2 * max_steps;
                 CK(cudaGetLastError());
                 CK(cudaMemcpyAsync(h, c->d_ctl, sizeof(Ctl), cudaMemcpyDeviceToHost, c->stream));

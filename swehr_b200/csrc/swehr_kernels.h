@@ -14,10 +14,21 @@ struct Bufs {
     const double *ks;
 };
 
+/* launch geometry of the step kernels of one simulation */
+struct StepConfig {
+    int grid_wave = 1, grid_update = 1;
+    size_t smem_wave = 0, smem_update = 0;
+    void *fn_update = nullptr;
+};
+
+/* Pick the kernel instantiation, set its shared-memory limit and size the
+ * persistent grids from the occupancy (returns a cudaError_t). */
+int configure_step_f64(const DevParams &P, int num_sms, StepConfig &cfg);
+
 /* Enqueue one full step (wave pass + update pass) of the FP64 form.
  * ev0/ev1 (optional) are recorded around the update kernel. */
 int launch_step_f64(const DevParams &P, const Bufs &B, Ctl *ctl, const double *rain, double *partials,
-                    double *stage, double *saveflow, int grid, cudaStream_t s, cudaEvent_t ev0, cudaEvent_t ev1);
-int step_grid_f64(const DevParams &P, int num_sms);
+                    double *stage, double *saveflow, const StepConfig &cfg, cudaStream_t s, cudaEvent_t ev0,
+                    cudaEvent_t ev1);
 
 }  // namespace swehr
