@@ -46,6 +46,12 @@ def algo_bytes_f64(S: int) -> int:
     return 16 * (7 + 2 * S) + 8
 
 
+def algo_bytes_mixed(S: int) -> int:
+    """Algorithmic bytes per cell-step of the mixed form: FP32 h, hu, hv,
+    MAXDEPTH, MAXVEL, U_k; FP64 z, VINF, M_k; FP32 Ks."""
+    return 2 * (4 * (5 + S) + 8 * (2 + S)) + 4
+
+
 def hbm_peak():
     try:
         with open(PEAKS_PATH) as f:
@@ -176,6 +182,7 @@ def main():
     ap.add_argument("--ny", type=int, default=4096)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-mixed", action="store_true")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
@@ -201,11 +208,10 @@ def main():
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
 
     from swehr_b200.lib import Simulation
+    from swehr_b200.params import FP64, MIXED
     case = bench_workload(args)
     S = case.sclass
     cells = case.cells()
-    sim = Simulation(case)
-    sim.advance(max_steps=args.warmup)
 
     def barrier():
         if dist is not None:
@@ -214,24 +220,49 @@ def main():
             dist.all_reduce(t)
             torch.cuda.synchronize()
 
+    def max_over_ranks(x: float) -> float:
+        if dist is None:
+            return x
+        import torch
+        t = torch.tensor([x], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    def timed_run(precision, clocks=None):
+        sim = Simulation(case, precision=precision)
+        sim.advance(max_steps=args.warmup)
+        barrier()
+        if clocks:
+            clocks.start()
+        sim.set_timing(True)
+        pr = sim.advance(max_steps=args.steps)
+        sim.set_timing(False)
+        clk = clocks.stop() if clocks else None
+        barrier()
+        sim.close()
+        return pr, clk
+
     clocks = ClockSampler(local)
-    barrier()
-    clocks.start()
-    sim.set_timing(True)
-    pr = sim.advance(max_steps=args.steps)
-    sim.set_timing(False)
-    clk = clocks.stop()
-    barrier()
-    elapsed_ms = pr.device_ms
+    pr, clk = timed_run(FP64, clocks)
+    elapsed_ms = max_over_ranks(pr.device_ms)
     kernel_ms = pr.kernel_ms
     steps_done = pr.steps_this_call
-    if dist is not None:
-        import torch
-        t = torch.tensor([elapsed_ms], device="cuda", dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        elapsed_ms = float(t.item())
     value = world * cells * steps_done / (elapsed_ms / 1e3)
-    sim.close()
+
+    mixed = None
+    if not args.no_mixed:
+        prm, _ = timed_run(MIXED)
+        em = max_over_ranks(prm.device_ms)
+        vm = world * cells * prm.steps_this_call / (em / 1e3)
+        um = prm.kernel_ms / max(prm.steps_this_call, 1)
+        Bm = algo_bytes_mixed(S)
+        mixed = {"value": vm, "unit": "cell-steps/s", "ms_per_step": em / max(prm.steps_this_call, 1),
+                 "steps": int(prm.steps_this_call), "gpu_launches": int(prm.kernel_launches),
+                 "over_fp64": vm / value,
+                 "roofline": {"bound": "hbm", "achieved": Bm * cells / (um / 1e3) / 1e9 if um > 0 else None,
+                              "unit": "GB/s", "algo_bytes_per_cell_step": Bm, "update_ms_avg": um},
+                 "dtype": "f32 bulk; f64 z, infiltration, deposited mass, budgets",
+                 "error_bar": "<=1e-4 relative L-inf on depth and concentration vs FP64 (tests/test_gpu_mixed.py)"}
 
     # end-to-end through the C ABI from host buffers: create (H2D of every
     # input) + the same steps + D2H of every output field, wall-clock
@@ -296,6 +327,7 @@ def main():
                          "algo_bytes_per_cell_step": B, "update_ms_avg": upd_ms},
             "cpu_baseline": cpu,
             "e2e": e2e,
+            "mixed_form": mixed,
             "clocks": clk,
             "gpu_launches": int(pr.kernel_launches),
             "impl": "swehr",

@@ -132,8 +132,8 @@ typedef struct swehr_progress {
 /* Water / sediment budget (an addition; the reference keeps none).  All sums
  * are over the interior cells in depth units [m] (water) or mass per area
  * [kg/m^2] (sediment, per class), accumulated in compensated FP64.
- * water:  sum(h+VINF)_now - sum(h+VINF)_0 == rain_in - outflow + clamp_gain + bulking
- * sed k:  sum(U_k+M_k)_now - sum(U_k+M_k)_0 == detach_k - sed_outflow_k */
+ * water:  sum(h+VINF)_now - sum(h+VINF)_0 == rain_in - outflow + clamp_gain + bulking + rounding
+ * sed k:  sum(U_k+M_k)_now - sum(U_k+M_k)_0 == detach_k - sed_outflow_k + sed_rounding_k */
 typedef struct swehr_budget {
     double water_now, water_init;
     double rain_in, outflow, clamp_gain, bulking, infiltration;
@@ -143,6 +143,11 @@ typedef struct swehr_budget {
     double sed_residual[SWEHR_MAX_CLASSES];
     int32_t sclass;
     int32_t valid;
+    /* rounding of the stored state: what the arithmetic and the storage format
+     * (FP32 in the mixed form) added to sum(h) and sum(U_k+M_k); ~1e-17
+     * relative in the plain form */
+    double rounding;
+    double sed_rounding[SWEHR_MAX_CLASSES];
 } swehr_budget;
 
 typedef struct swehr_ctx swehr_ctx;

@@ -25,6 +25,7 @@ COMMON = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-I", CSRC, "
 # (source, extra flags)
 SOURCES = [
     ("swehr_step_f64.cu", ["--fmad=false"]),
+    ("swehr_step_f32.cu", []),
     ("swehr_capi.cu", []),
     ("swehr_cfl_noalloc.cu", ["--fmad=false"]),
 ]

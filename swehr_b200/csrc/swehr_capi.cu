@@ -46,7 +46,9 @@ struct swehr_ctx {
     int precision = SWEHR_FP64;
     int device = 0, num_sms = 148;
     DevParams P;
-    Bufs B;
+    BufsT<double> B64;      /* plain form */
+    BufsT<float> B32;       /* mixed form */
+    size_t rsize = 8;       /* bytes of a bulk (RS) element */
     char *pool = nullptr;
     size_t pool_bytes = 0;
     double *d_rain = nullptr, *d_partials = nullptr, *d_stage = nullptr, *d_saveflow = nullptr;
@@ -117,23 +119,28 @@ void swehr_set_last_error(const char *msg) { g_last_error = msg ? msg : ""; }
 
 static int64_t round_up(int64_t x, int64_t m) { return (x + m - 1) / m * m; }
 
+/* Device layout of one simulation.  A state set is, in the plain form, 9 + 2S
+ * double planes in the order h hu hv vinf maxvel maxdep totm dep totsed
+ * U_1..U_S M_1..M_S; in the mixed form 8 + S float planes (h hu hv maxvel
+ * maxdep totm dep totsed U_1..U_S) followed by 1 + S double planes (vinf
+ * M_1..M_S).  Then three double z planes, the Ks plane (bulk type), rain,
+ * control block, reduction partials and stage rows. */
 struct Layout {
-    int64_t pitch, plane, np, nplanes;
-    size_t bytes_state, off_z, off_ks, off_rain, off_ctl, off_partials, off_stage, off_saveflow, total;
+    int64_t pitch, plane;
+    size_t rsize, set_bytes, off_z, off_ks, off_rain, off_ctl, off_partials, off_stage, off_saveflow, total;
 };
 
-static Layout layout_for(int nx, int ny, int S, int rnum, int has_ks, int64_t stagecap, int grid)
+static Layout layout_for(int nx, int ny, int S, int rnum, int has_ks, int64_t stagecap, int grid, int precision)
 {
     Layout L;
     L.pitch = round_up(ny, 32);
     L.plane = round_up((int64_t)nx * L.pitch, 32);
-    L.np = P_FIXED + 2 * S;
-    L.nplanes = 2 * L.np + 3 + (has_ks ? 1 : 0);
-    size_t pb = (size_t)L.plane * sizeof(double);
-    L.bytes_state = 2 * L.np * pb;
-    L.off_z = L.bytes_state;
+    L.rsize = precision == SWEHR_MIXED ? sizeof(float) : sizeof(double);
+    const size_t pb = (size_t)L.plane * sizeof(double), pr = (size_t)L.plane * L.rsize;
+    L.set_bytes = precision == SWEHR_MIXED ? (size_t)(8 + S) * pr + (size_t)(1 + S) * pb : (size_t)(P_FIXED + 2 * S) * pb;
+    L.off_z = 2 * L.set_bytes;
     L.off_ks = L.off_z + 3 * pb;
-    L.off_rain = L.off_ks + (has_ks ? pb : 0);
+    L.off_rain = L.off_ks + (has_ks ? pr : 0);
     L.off_ctl = (size_t)round_up((int64_t)(L.off_rain + (size_t)rnum * sizeof(double)), 256);
     L.off_partials = (size_t)round_up((int64_t)(L.off_ctl + sizeof(Ctl)), 256);
     L.off_stage = (size_t)round_up((int64_t)(L.off_partials + (size_t)grid * B_NTERMS * sizeof(double)), 256);
@@ -151,8 +158,7 @@ static int64_t stagecap_for(const swehr_params *p)
 
 extern "C" size_t swehr_footprint_bytes(int nx, int ny, int sclass, int precision)
 {
-    (void)precision;
-    return layout_for(nx, ny, sclass, 64, 1, 4096, 148 * 4).total;
+    return layout_for(nx, ny, sclass, 64, 1, 4096, 148 * 4, precision).total;
 }
 
 static int validate(const swehr_params *p, const swehr_inputs *in)
@@ -169,6 +175,21 @@ static int validate(const swehr_params *p, const swehr_inputs *in)
     if (p->storm_peak > 0 && !(p->storm_radius > 0)) return set_err(SWEHR_INVALID, "storm_radius must be > 0");
     if (!in->topo || !in->rain || !in->ds || !in->pfrac) return set_err(SWEHR_INVALID, "NULL input array");
     return SWEHR_OK;
+}
+
+template <class R>
+static void fill_realc(const DevParams &P, RealC<R> &K)
+{
+    K.g = (R)P.g; K.hfilm = (R)P.hfilm; K.hfx10 = (R)P.hfx10; K.rhos = (R)P.rhos; K.rhow = (R)P.rhow;
+    K.rho0 = (R)P.rho0; K.porod = (R)P.porod; K.oneoverdx = (R)P.oneoverdx; K.half_odx = (R)P.half_odx;
+    K.fa = (R)P.fa; K.cohesion = (R)P.cohesion; K.neg1ml = (R)P.neg1ml; K.cthreshold = (R)P.cthreshold;
+    K.one_m_bb = (R)P.one_m_bb; K.hc = (R)P.hc; K.dde = (R)P.dde; K.b = (R)P.b; K.af = (R)P.af; K.afr = (R)P.afr;
+    K.h0 = (R)P.h0; K.h0x3 = (R)P.h0x3; K.h0x6 = (R)P.h0x6; K.h0x9 = (R)P.h0x9; K.mtstar0 = (R)P.mtstar0;
+    K.a = (R)P.a; K.ad = (R)P.ad; K.F = (R)P.F; K.J = (R)P.J; K.roughness = (R)P.roughness;
+    K.uc = (R)P.uc; K.uc2 = (R)P.uc2; K.c109s = (R)P.c109s; K.rhos08 = (R)P.rhos08;
+    for (int k = 0; k < 16; k++) {
+        K.ds[k] = (R)P.ds[k]; K.pf[k] = (R)P.pf[k]; K.a13[k] = (R)P.a13[k]; K.a13sq[k] = (R)P.a13sq[k];
+    }
 }
 
 static void make_devparams(const swehr_params *p, const swehr_inputs *in, const Layout &L, DevParams &P)
@@ -204,20 +225,74 @@ static void make_devparams(const swehr_params *p, const swehr_inputs *in, const 
         P.a13[k] = 13.95 * p->nu / in->ds[k];
         P.a13sq[k] = P.a13[k] * P.a13[k];
     }
+    fill_realc(P, P.kd);
+    fill_realc(P, P.kf);
 }
 
-static int upload_plane(swehr_ctx *c, double *dplane, const double *host, cudaStream_t s)
+/* one device plane: element size 8 (double) or 4 (float) */
+struct PlaneRef {
+    void *ptr;
+    size_t esize;
+};
+
+static int upload_plane(swehr_ctx *c, PlaneRef d, const double *host, cudaStream_t s)
 {
-    CK(cudaMemcpy2DAsync(dplane, (size_t)c->P.pitch * sizeof(double), host, (size_t)c->P.ny * sizeof(double),
-                         (size_t)c->P.ny * sizeof(double), (size_t)c->P.nx, cudaMemcpyHostToDevice, s));
+    const size_t N = (size_t)c->P.nx * c->P.ny;
+    if (d.esize == sizeof(double)) {
+        CK(cudaMemcpy2DAsync(d.ptr, (size_t)c->P.pitch * sizeof(double), host, (size_t)c->P.ny * sizeof(double),
+                             (size_t)c->P.ny * sizeof(double), (size_t)c->P.nx, cudaMemcpyHostToDevice, s));
+        return SWEHR_OK;
+    }
+    std::vector<float> tmp(N);
+    for (size_t q = 0; q < N; q++) tmp[q] = (float)host[q];
+    CK(cudaMemcpy2DAsync(d.ptr, (size_t)c->P.pitch * sizeof(float), tmp.data(), (size_t)c->P.ny * sizeof(float),
+                         (size_t)c->P.ny * sizeof(float), (size_t)c->P.nx, cudaMemcpyHostToDevice, s));
+    CK(cudaStreamSynchronize(s));
     return SWEHR_OK;
 }
 
-static int download_plane(swehr_ctx *c, double *host, const double *dplane, cudaStream_t s)
+static int download_plane(swehr_ctx *c, double *host, PlaneRef d, cudaStream_t s)
 {
-    CK(cudaMemcpy2DAsync(host, (size_t)c->P.ny * sizeof(double), dplane, (size_t)c->P.pitch * sizeof(double),
-                         (size_t)c->P.ny * sizeof(double), (size_t)c->P.nx, cudaMemcpyDeviceToHost, s));
+    const size_t N = (size_t)c->P.nx * c->P.ny;
+    if (d.esize == sizeof(double)) {
+        CK(cudaMemcpy2DAsync(host, (size_t)c->P.ny * sizeof(double), d.ptr, (size_t)c->P.pitch * sizeof(double),
+                             (size_t)c->P.ny * sizeof(double), (size_t)c->P.nx, cudaMemcpyDeviceToHost, s));
+        return SWEHR_OK;
+    }
+    std::vector<float> tmp(N);
+    CK(cudaMemcpy2DAsync(tmp.data(), (size_t)c->P.ny * sizeof(float), d.ptr, (size_t)c->P.pitch * sizeof(float),
+                         (size_t)c->P.ny * sizeof(float), (size_t)c->P.nx, cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
+    for (size_t q = 0; q < N; q++) host[q] = (double)tmp[q];
     return SWEHR_OK;
+}
+
+template <class RS>
+static void set_views(BufsT<RS> &B, char *pool, const Layout &L, int S, int has_ks, int mixed)
+{
+    for (int s = 0; s < 2; s++) {
+        char *base = pool + (size_t)s * L.set_bytes;
+        SetV<RS> &v = B.set[s];
+        const int64_t pl = L.plane;
+        if (!mixed) {
+            double *d = (double *)base;
+            v.h = (RS *)(d + P_H * pl); v.hu = (RS *)(d + P_HU * pl); v.hv = (RS *)(d + P_HV * pl);
+            v.vinf = d + P_VINF * pl;
+            v.maxvel = (RS *)(d + P_MAXVEL * pl); v.maxdep = (RS *)(d + P_MAXDEP * pl);
+            v.totm = (RS *)(d + P_TOTM * pl); v.dep = (RS *)(d + P_DEP * pl); v.totsed = (RS *)(d + P_TOTSED * pl);
+            v.U = (RS *)(d + P_FIXED * pl);
+            v.M = d + (P_FIXED + S) * pl;
+        } else {
+            RS *f = (RS *)base;
+            v.h = f; v.hu = f + pl; v.hv = f + 2 * pl; v.maxvel = f + 3 * pl; v.maxdep = f + 4 * pl;
+            v.totm = f + 5 * pl; v.dep = f + 6 * pl; v.totsed = f + 7 * pl; v.U = f + 8 * pl;
+            double *d = (double *)(base + (size_t)(8 + S) * pl * sizeof(RS));
+            v.vinf = d;
+            v.M = d + pl;
+        }
+    }
+    for (int k = 0; k < 3; k++) B.z[k] = (double *)(pool + L.off_z) + k * L.plane;
+    B.ks = has_ks ? (const RS *)(pool + L.off_ks) : nullptr;
 }
 
 static void destroy_ctx(swehr_ctx *c)
@@ -241,7 +316,7 @@ extern "C" int swehr_create(const swehr_params *p, const swehr_inputs *in, int p
     *out = nullptr;
     int v = validate(p, in);
     if (v) return v;
-    if (precision != SWEHR_FP64) return set_err(SWEHR_INVALID, "precision not supported by this build");
+    if (precision != SWEHR_FP64 && precision != SWEHR_MIXED) return set_err(SWEHR_INVALID, "unknown precision");
     int ndev = 0;
     if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev < 1) return set_err(SWEHR_NO_DEVICE, "no CUDA device");
     swehr_ctx *c = new swehr_ctx();
@@ -262,27 +337,27 @@ extern "C" int swehr_create(const swehr_params *p, const swehr_inputs *in, int p
     CKC(cudaDeviceGetAttribute(&c->num_sms, cudaDevAttrMultiProcessorCount, c->device));
     c->stagecap = stagecap_for(p);
     DevParams tmpP;
-    Layout L0 = layout_for(p->nx, p->ny, p->sclass, p->rnum, in->ks != nullptr, c->stagecap, 1);
+    Layout L0 = layout_for(p->nx, p->ny, p->sclass, p->rnum, in->ks != nullptr, c->stagecap, 1, precision);
     make_devparams(p, in, L0, tmpP);
     {
-        int ce = configure_step_f64(tmpP, c->num_sms, c->cfg);
+        int ce = precision == SWEHR_MIXED ? configure_step_f32(tmpP, c->num_sms, c->cfg)
+                                          : configure_step_f64(tmpP, c->num_sms, c->cfg);
         if (ce) {
             rc = set_err(SWEHR_CUDA_ERROR, std::string("configure: ") + cudaGetErrorString((cudaError_t)ce));
             destroy_ctx(c);
             return rc;
         }
     }
-    Layout L = layout_for(p->nx, p->ny, p->sclass, p->rnum, in->ks != nullptr, c->stagecap, c->cfg.grid_update);
+    Layout L = layout_for(p->nx, p->ny, p->sclass, p->rnum, in->ks != nullptr, c->stagecap, c->cfg.grid_update,
+                          precision);
+    c->rsize = L.rsize;
     make_devparams(p, in, L, c->P);
     CKC(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
     CKC(cudaMalloc((void **)&c->pool, L.total));
     c->pool_bytes = L.total;
     CKC(cudaMemsetAsync(c->pool, 0, L.total, c->stream));
-    double *base = (double *)c->pool;
-    c->B.set[0] = base;
-    c->B.set[1] = base + L.np * L.plane;
-    for (int k = 0; k < 3; k++) c->B.z[k] = (double *)(c->pool + L.off_z) + k * L.plane;
-    c->B.ks = in->ks ? (const double *)(c->pool + L.off_ks) : nullptr;
+    if (precision == SWEHR_MIXED) set_views(c->B32, c->pool, L, p->sclass, in->ks != nullptr, 1);
+    else set_views(c->B64, c->pool, L, p->sclass, in->ks != nullptr, 0);
     c->d_rain = (double *)(c->pool + L.off_rain);
     c->d_ctl = (Ctl *)(c->pool + L.off_ctl);
     c->d_partials = (double *)(c->pool + L.off_partials);
@@ -294,20 +369,22 @@ extern "C" int swehr_create(const swehr_params *p, const swehr_inputs *in, int p
     for (int e = 0; e < 2 * TIMING_RING; e++) CKC(cudaEventCreate(&c->ev_k[e]));
     /* initial state (initialcondition, SWEHR.c:211-285): dry bed, VINF = vinf0, z = topo;
      * z of the previous step = z (setup slopes, SWEHR.c:721-803) */
+    double *const *zpl = precision == SWEHR_MIXED ? c->B32.z : c->B64.z;
     for (int k = 0; k < 3; k++) {
-        rc = upload_plane(c, c->B.z[k], in->topo, c->stream);
+        rc = upload_plane(c, PlaneRef{zpl[k], sizeof(double)}, in->topo, c->stream);
         if (rc) { destroy_ctx(c); return rc; }
     }
     if (in->ks) {
-        rc = upload_plane(c, (double *)c->B.ks, in->ks, c->stream);
+        void *kp = precision == SWEHR_MIXED ? (void *)c->B32.ks : (void *)c->B64.ks;
+        rc = upload_plane(c, PlaneRef{kp, L.rsize}, in->ks, c->stream);
         if (rc) { destroy_ctx(c); return rc; }
     }
     {
         std::vector<double> row((size_t)c->P.plane, 0.0);
         for (int i = 0; i < p->nx; i++)
             for (int j = 0; j < p->ny; j++) row[(size_t)i * c->P.pitch + j] = p->vinf0;
-        CKC(cudaMemcpyAsync(c->B.set[0] + P_VINF * c->P.plane, row.data(), (size_t)c->P.plane * sizeof(double),
-                            cudaMemcpyHostToDevice, c->stream));
+        double *vinf0 = precision == SWEHR_MIXED ? c->B32.set[0].vinf : c->B64.set[0].vinf;
+        CKC(cudaMemcpyAsync(vinf0, row.data(), (size_t)c->P.plane * sizeof(double), cudaMemcpyHostToDevice, c->stream));
         CKC(cudaMemcpyAsync(c->d_rain, in->rain, (size_t)p->rnum * sizeof(double), cudaMemcpyHostToDevice, c->stream));
         Ctl h;
         memset(&h, 0, sizeof h);
@@ -333,14 +410,21 @@ extern "C" int swehr_set_timing(swehr_ctx *c, int on)
     return SWEHR_OK;
 }
 
+static int launch_step(swehr_ctx *c, cudaEvent_t ev0, cudaEvent_t ev1)
+{
+    if (c->precision == SWEHR_MIXED)
+        return launch_step_f32(c->P, c->B32, c->d_ctl, c->d_rain, c->d_partials, c->d_stage, c->d_saveflow, c->cfg,
+                               c->stream, ev0, ev1);
+    return launch_step_f64(c->P, c->B64, c->d_ctl, c->d_rain, c->d_partials, c->d_stage, c->d_saveflow, c->cfg,
+                           c->stream, ev0, ev1);
+}
+
 static int build_graph(swehr_ctx *c)
 {
     if (c->graph) return SWEHR_OK;
     cudaGraph_t g;
     CK(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
-    for (int s = 0; s < GRAPH_STEPS; s++)
-        launch_step_f64(c->P, c->B, c->d_ctl, c->d_rain, c->d_partials, c->d_stage, c->d_saveflow, c->cfg,
-                        c->stream, nullptr, nullptr);
+    for (int s = 0; s < GRAPH_STEPS; s++) launch_step(c, nullptr, nullptr);
     CK(cudaStreamEndCapture(c->stream, &g));
     cudaError_t e = cudaGraphInstantiate(&c->graph, g, 0);
     cudaGraphDestroy(g);
@@ -380,8 +464,7 @@ extern "C" int swehr_advance(swehr_ctx *c, double t_stop, int64_t max_steps, swe
                 int n = TIMING_RING;
                 if (max_steps >= 0 && left < n) n = (int)left;
                 for (int s = 0; s < n; s++) {
-                    int e = launch_step_f64(c->P, c->B, c->d_ctl, c->d_rain, c->d_partials, c->d_stage, c->d_saveflow,
-                                            c->cfg, c->stream, c->ev_k[2 * s], c->ev_k[2 * s + 1]);
+                    int e = launch_step(c, c->ev_k[2 * s], c->ev_k[2 * s + 1]);
                     if (e) return set_err(SWEHR_CUDA_ERROR, std::string("launch: ") + cudaGetErrorString((cudaError_t)e));
                 }
                 launched += 2 * n;
@@ -401,9 +484,7 @@ extern "C" int swehr_advance(swehr_ctx *c, double t_stop, int64_t max_steps, swe
             if (max_steps >= 0) {
                 int64_t full = max_steps / GRAPH_STEPS, rem = max_steps % GRAPH_STEPS;
                 for (int64_t gi = 0; gi < full; gi++) CK(cudaGraphLaunch(c->graph, c->stream));
-                for (int64_t s = 0; s < rem; s++)
-                    launch_step_f64(c->P, c->B, c->d_ctl, c->d_rain, c->d_partials, c->d_stage, c->d_saveflow,
-                                    c->cfg, c->stream, nullptr, nullptr);
+                for (int64_t s = 0; s < rem; s++) launch_step(c, nullptr, nullptr);
                 launched = 2 * max_steps;
                 CK(cudaGetLastError());
                 CK(cudaMemcpyAsync(h, c->d_ctl, sizeof(Ctl), cudaMemcpyDeviceToHost, c->stream));
@@ -440,24 +521,37 @@ extern "C" int swehr_advance(swehr_ctx *c, double t_stop, int64_t max_steps, swe
     return st;
 }
 
-static double *field_plane(swehr_ctx *c, int field, int k, int cur)
+template <class RS>
+static PlaneRef field_plane_t(const BufsT<RS> &B, int field, int k, int cur, int64_t pl)
 {
-    double *set = c->B.set[cur];
-    int64_t pl = c->P.plane;
+    const SetV<RS> &v = B.set[cur];
+    const size_t r = sizeof(RS), d = sizeof(double);
     switch (field) {
-    case SWEHR_FIELD_H: return set + P_H * pl;
-    case SWEHR_FIELD_HU: return set + P_HU * pl;
-    case SWEHR_FIELD_HV: return set + P_HV * pl;
-    case SWEHR_FIELD_VINF: return set + P_VINF * pl;
-    case SWEHR_FIELD_MAXVEL: return set + P_MAXVEL * pl;
-    case SWEHR_FIELD_MAXDEPTH: return set + P_MAXDEP * pl;
-    case SWEHR_FIELD_TOTM: return set + P_TOTM * pl;
-    case SWEHR_FIELD_DEP: return set + P_DEP * pl;
-    case SWEHR_FIELD_TOTSED: return set + P_TOTSED * pl;
-    case SWEHR_FIELD_U: return set + (P_FIXED + k - 1) * pl;
-    case SWEHR_FIELD_M: return set + (P_FIXED + c->P.S + k - 1) * pl;
-    default: return nullptr;
+    case SWEHR_FIELD_H: return PlaneRef{v.h, r};
+    case SWEHR_FIELD_HU: return PlaneRef{v.hu, r};
+    case SWEHR_FIELD_HV: return PlaneRef{v.hv, r};
+    case SWEHR_FIELD_VINF: return PlaneRef{v.vinf, d};
+    case SWEHR_FIELD_MAXVEL: return PlaneRef{v.maxvel, r};
+    case SWEHR_FIELD_MAXDEPTH: return PlaneRef{v.maxdep, r};
+    case SWEHR_FIELD_TOTM: return PlaneRef{v.totm, r};
+    case SWEHR_FIELD_DEP: return PlaneRef{v.dep, r};
+    case SWEHR_FIELD_TOTSED: return PlaneRef{v.totsed, r};
+    case SWEHR_FIELD_U: return PlaneRef{v.U + (k - 1) * pl, r};
+    case SWEHR_FIELD_M: return PlaneRef{v.M + (k - 1) * pl, d};
+    default: return PlaneRef{nullptr, 0};
     }
+}
+
+static PlaneRef field_plane(swehr_ctx *c, int field, int k, int cur)
+{
+    if (c->precision == SWEHR_MIXED) return field_plane_t(c->B32, field, k, cur, c->P.plane);
+    return field_plane_t(c->B64, field, k, cur, c->P.plane);
+}
+
+static PlaneRef z_plane(swehr_ctx *c, int64_t m)
+{
+    double *const *z = c->precision == SWEHR_MIXED ? c->B32.z : c->B64.z;
+    return PlaneRef{z[m % 3], sizeof(double)};
 }
 
 static int current_step(swehr_ctx *c, int64_t *step)
@@ -481,7 +575,7 @@ extern "C" int swehr_read_field(swehr_ctx *c, int field, int k, double *dst)
     const size_t N = (size_t)c->P.nx * c->P.ny;
     const double hfilm = c->P.hfilm;
     if (field == SWEHR_FIELD_Z) {
-        rc = download_plane(c, dst, c->B.z[step % 3], c->stream);
+        rc = download_plane(c, dst, z_plane(c, step), c->stream);
     } else if (field == SWEHR_FIELD_VEL || field == SWEHR_FIELD_SED) {
         std::vector<double> h(N), a(N), b(N);
         rc = download_plane(c, h.data(), field_plane(c, SWEHR_FIELD_H, 0, cur), c->stream);
@@ -501,8 +595,8 @@ extern "C" int swehr_read_field(swehr_ctx *c, int field, int k, double *dst)
         }
         return SWEHR_OK;
     } else {
-        double *src = field_plane(c, field, k, cur);
-        if (!src) return set_err(SWEHR_INVALID, "unknown field");
+        PlaneRef src = field_plane(c, field, k, cur);
+        if (!src.ptr) return set_err(SWEHR_INVALID, "unknown field");
         rc = download_plane(c, dst, src, c->stream);
     }
     if (rc) return rc;
@@ -518,14 +612,14 @@ extern "C" int swehr_write_field(swehr_ctx *c, int field, int k, const double *s
     if (rc) return rc;
     const int cur = (int)(step & 1);
     if (field == SWEHR_FIELD_Z) {
-        rc = upload_plane(c, c->B.z[step % 3], src, c->stream);
-        if (!rc) rc = upload_plane(c, c->B.z[(step + 2) % 3], src, c->stream);
+        rc = upload_plane(c, z_plane(c, step), src, c->stream);
+        if (!rc) rc = upload_plane(c, z_plane(c, step + 2), src, c->stream);
     } else {
         if ((field == SWEHR_FIELD_U || field == SWEHR_FIELD_M) && (k < 1 || k > c->P.S))
             return set_err(SWEHR_INVALID, "class index out of range");
         if (field == SWEHR_FIELD_VEL || field == SWEHR_FIELD_SED) return set_err(SWEHR_INVALID, "derived field");
-        double *dstp = field_plane(c, field, k, cur);
-        if (!dstp) return set_err(SWEHR_INVALID, "unknown field");
+        PlaneRef dstp = field_plane(c, field, k, cur);
+        if (!dstp.ptr) return set_err(SWEHR_INVALID, "unknown field");
         rc = upload_plane(c, dstp, src, c->stream);
     }
     if (rc) return rc;
@@ -581,7 +675,8 @@ extern "C" int swehr_get_budget(swehr_ctx *c, swehr_budget *b)
     b->clamp_gain = term(B_CLAMP);
     b->bulking = term(B_BULK);
     b->infiltration = term(B_INF);
-    b->water_residual = (wsum - c->water_init) - (b->rain_in - b->outflow + b->clamp_gain + b->bulking);
+    b->rounding = term(B_ROUND);
+    b->water_residual = (wsum - c->water_init) - (b->rain_in - b->outflow + b->clamp_gain + b->bulking + b->rounding);
     b->sclass = c->P.S;
     for (int k = 0; k < c->P.S; k++) {
         rc = swehr_read_field(c, SWEHR_FIELD_U, k + 1, tmp.data());
@@ -592,7 +687,8 @@ extern "C" int swehr_get_budget(swehr_ctx *c, swehr_budget *b)
         b->sed_init[k] = c->sed_init[k];
         b->detach[k] = term(B_DET + k);
         b->sed_outflow[k] = term(B_SOUT + k);
-        b->sed_residual[k] = (s - c->sed_init[k]) - (b->detach[k] - b->sed_outflow[k]);
+        b->sed_rounding[k] = term(B_SROUND + k);
+        b->sed_residual[k] = (s - c->sed_init[k]) - (b->detach[k] - b->sed_outflow[k] + b->sed_rounding[k]);
     }
     b->valid = c->P.budget;
     return SWEHR_OK;

@@ -25,6 +25,16 @@ namespace swehr {
 
 enum { P_H = 0, P_HU, P_HV, P_VINF, P_MAXVEL, P_MAXDEP, P_TOTM, P_DEP, P_TOTSED, P_FIXED };
 
+/* Real-valued constants of the step in the arithmetic type R of a form
+ * (double for the plain form, float for the mixed form's bulk). */
+template <class R>
+struct RealC {
+    R g, hfilm, hfx10, rhos, rhow, rho0, porod, oneoverdx, half_odx;
+    R fa, cohesion, neg1ml, cthreshold, one_m_bb, hc, dde, b, af, afr;
+    R h0, h0x3, h0x6, h0x9, mtstar0, a, ad, F, J, roughness, uc, uc2, c109s, rhos08;
+    R ds[16], pf[16], a13[16], a13sq[16];
+};
+
 struct DevParams {
     int32_t nx, ny, S, pitch;
     int32_t rnum, inflow, storm, budget;
@@ -41,7 +51,16 @@ struct DevParams {
     double rhos08;        /* 0.8*rhos */
     double storm_peak, storm_r2, storm_x0, storm_y0, storm_vx, storm_vy;
     double ds[16], pf[16], a13[16], a13sq[16];
+    RealC<double> kd;     /* the constants above, for templated kernels */
+    RealC<float> kf;      /* the same, rounded to float, for the mixed form */
 };
+
+template <class R>
+__device__ __forceinline__ const RealC<R> &kc(const DevParams &P);
+template <>
+__device__ __forceinline__ const RealC<double> &kc<double>(const DevParams &P) { return P.kd; }
+template <>
+__device__ __forceinline__ const RealC<float> &kc<float>(const DevParams &P) { return P.kf; }
 
 /* Device control block of one simulation (one per scenario). */
 struct Ctl {
@@ -59,12 +78,19 @@ struct Ctl {
     double stageinterval;
     int64_t stagecnt, stagecap;
     int64_t launches;
-    double budget_hi[48], budget_lo[48];   /* running compensated budget sums */
+    double budget_hi[64], budget_lo[64];   /* running compensated budget sums */
     double sed0[16];
 };
 
 /* budget term slots */
-enum { B_RAIN = 0, B_OUT, B_CLAMP, B_BULK, B_INF, B_DET = 5 /* +k */, B_SOUT = 5 + 16 /* +k */, B_NTERMS = 5 + 32 };
+enum {
+    B_RAIN = 0, B_OUT, B_CLAMP, B_BULK, B_INF,
+    B_ROUND,                  /* storage/arithmetic rounding of h (the mixed form's FP32 representation) */
+    B_DET = 6,                /* + class */
+    B_SOUT = 6 + 16,          /* + class */
+    B_SROUND = 6 + 32,        /* + class: rounding of U_k + M_k */
+    B_NTERMS = 6 + 48
+};
 
 __device__ __forceinline__ int64_t cidx(const DevParams &P, int i, int j)
 {

@@ -6,28 +6,41 @@
 
 namespace swehr {
 
-/* device buffers of one simulation: two state sets (9 + 2S planes each),
- * three topography planes, optional per-cell Ks */
-struct Bufs {
-    double *set[2];
+/* one state set as seen by a kernel: RS = storage type of the bulk fields
+ * (double in the plain form, float in the mixed form) */
+template <class RS>
+struct SetV {
+    RS *h, *hu, *hv, *maxvel, *maxdep, *totm, *dep, *totsed, *U;   /* U: S planes */
+    double *vinf, *M;                                                /* M: S planes */
+};
+
+/* device buffers of one simulation: two state sets, the topography of the
+ * previous, current and next step, optional per-cell Ks */
+template <class RS>
+struct BufsT {
+    SetV<RS> set[2];
     double *z[3];
-    const double *ks;
+    const RS *ks;
 };
 
 /* launch geometry of the step kernels of one simulation */
 struct StepConfig {
     int grid_wave = 1, grid_update = 1;
     size_t smem_wave = 0, smem_update = 0;
-    void *fn_update = nullptr;
+    void *fn_update = nullptr, *fn_wave = nullptr;
 };
 
-/* Pick the kernel instantiation, set its shared-memory limit and size the
- * persistent grids from the occupancy (returns a cudaError_t). */
+/* Pick the kernel instantiations, set their shared-memory limit and size the
+ * persistent grids from the occupancy (return a cudaError_t). */
 int configure_step_f64(const DevParams &P, int num_sms, StepConfig &cfg);
+int configure_step_f32(const DevParams &P, int num_sms, StepConfig &cfg);
 
-/* Enqueue one full step (wave pass + update pass) of the FP64 form.
- * ev0/ev1 (optional) are recorded around the update kernel. */
-int launch_step_f64(const DevParams &P, const Bufs &B, Ctl *ctl, const double *rain, double *partials,
+/* Enqueue one full step (wave pass + update pass); ev0/ev1 (optional) are
+ * recorded around the update kernel. */
+int launch_step_f64(const DevParams &P, const BufsT<double> &B, Ctl *ctl, const double *rain, double *partials,
+                    double *stage, double *saveflow, const StepConfig &cfg, cudaStream_t s, cudaEvent_t ev0,
+                    cudaEvent_t ev1);
+int launch_step_f32(const DevParams &P, const BufsT<float> &B, Ctl *ctl, const double *rain, double *partials,
                     double *stage, double *saveflow, const StepConfig &cfg, cudaStream_t s, cudaEvent_t ev0,
                     cudaEvent_t ev1);
 

@@ -1,0 +1,24 @@
+/*
+ * swehr_step_f32.cu -- the mixed form of one SWEHR time step on sm_100a:
+ * h, hu, hv, U_k, the maxima, TOTM, DEP, TOTSED and Ks in FP32 (SFU
+ * intrinsics, fused multiply-add allowed); z, cumulative infiltration and its
+ * Green-Ampt update, deposited mass M_k, t/dt and the budgets in FP64.
+ * Same two-launch step as the FP64 form (swehr_step_f64.cu).
+ */
+#include "swehr_launch.cuh"
+
+namespace swehr {
+
+int configure_step_f32(const DevParams &P, int num_sms, StepConfig &cfg)
+{
+    return FormLauncher<PolicyF32, float>::configure(P, num_sms, cfg);
+}
+
+int launch_step_f32(const DevParams &P, const BufsT<float> &B, Ctl *ctl, const double *rain, double *partials,
+                    double *stage, double *saveflow, const StepConfig &cfg, cudaStream_t s, cudaEvent_t ev0,
+                    cudaEvent_t ev1)
+{
+    return FormLauncher<PolicyF32, float>::launch(P, B, ctl, rain, partials, stage, saveflow, cfg, s, ev0, ev1);
+}
+
+}  // namespace swehr

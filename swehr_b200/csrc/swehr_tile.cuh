@@ -1,5 +1,13 @@
 /*
- * swehr_tile.cuh -- tiled kernels of one SWEHR time step (FP64 form).
+ * swehr_tile.cuh -- tiled kernels of one SWEHR time step, templated on the
+ * arithmetic of the form:
+ *   PolicyF64  plain form: every value FP64, elementary functions from
+ *              swehr_math.h; with --fmad=false bit-identical to the CPU
+ *              restatement built with the same math;
+ *   PolicyF32  mixed form: h, hu, hv, U_k, the maxima, TOTM, DEP, TOTSED and
+ *              Ks stored and computed in FP32 with the SFU intrinsics; z, the
+ *              cumulative infiltration and its Green-Ampt update, the
+ *              deposited mass M_k, dt/t and the budgets stay FP64.
  *
  * A CTA of 256 threads owns 8 x 32 cells (i x j, j contiguous in HBM) and
  * loops over tiles (persistent grid).  Per tile:
@@ -13,8 +21,6 @@
  *   C. one thread per cell: sources (SWEHR.c:1239-1401), the conservative,
  *      Green-Ampt and class updates (SWEHR.c:1424-1511), the dry clamp,
  *      friction and maxima (SWEHR.c:1513-1588).
- * Every value is produced by the same operations in the same order as the
- * CPU restatement, so the FP64 results are bit-identical to it.
  *
  * The slope-failure test (SWEHR.c:1292-1312) costs six cos/sin(atan) and
  * neighbour slopes per cell but can only fire on steep, thick deposits: a
@@ -25,6 +31,9 @@
 #pragma once
 #include "swehr_device.cuh"
 #include "swehr_faces.cuh"
+#include "swehr_kernels.h"
+
+#include <cuda_pipeline_primitives.h>
 
 namespace swehr {
 
@@ -37,66 +46,91 @@ namespace swehr {
 #define N_FY (T_I * (T_J + 1))
 #define TILE_THREADS 256
 
-/* shared-memory layout of one tile (doubles), S classes */
-struct TileLayout {
-    int h, u, v, g, c, ts, dep, sed, fx, fy, up, red, total;
-    __host__ __device__ static TileLayout make(int S)
+/* ------------------------------------------------------------ policies --- */
+struct PolicyF64 {
+    typedef double R;
+    static constexpr int kMinBlocks = 2;      /* CTAs per SM the update kernel is register-budgeted for */
+    static __device__ __forceinline__ R sqrtp(R x) { return sw_sqrt_pow(x); }
+    static __device__ __forceinline__ R pow(R x, R y) { return sw_pow(x, y); }
+    static __device__ __forceinline__ R exp(R x) { return sw_exp(x); }
+    static __device__ __forceinline__ R cos_atan(R x) { return sw_cos_atan(x); }
+    static __device__ __forceinline__ R sin_atan(R x) { return sw_sin_atan(x); }
+    static __device__ __forceinline__ R div(R a, R b) { return a / b; }
+    static __device__ __forceinline__ R qnan() { return __longlong_as_double(0x7ff8000000000000LL); }
+    /* settling velocity of Cao 2006 (SWEHR.c:435): sqrt(A^2 + c) - A, in the
+     * reference's operation order */
+    static __device__ __forceinline__ R settle(R A, R A2, R c) { return sqrtp(A2 + c) - A; }
+};
+
+struct PolicyF32 {
+    typedef float R;
+    static constexpr int kMinBlocks = 3;
+    static __device__ __forceinline__ R sqrtp(R x)
     {
-        TileLayout L;
-        int o = 0;
-        L.h = o; o += N_H;
-        L.u = o; o += N_H;
-        L.v = o; o += N_H;
-        L.g = o; o += N_H;
-        L.c = o; o += N_H;
-        L.ts = o; o += N_H;
-        L.dep = o; o += N_H;
-        L.sed = o; o += S * N_H;
-        L.fx = o; o += 3 * N_FX;
-        L.fy = o; o += 3 * N_FY;
-        L.up = o; o += (N_FX + N_FY + 7) / 8;          /* one byte per face */
-        L.red = o; o += (TILE_THREADS / 32) * B_NTERMS;
-        L.total = o;
-        return L;
+        const float r = __fsqrt_rn(x);
+        return (r == 0.f) ? 0.f : r;
     }
+    static __device__ __forceinline__ R pow(R x, R y)
+    {
+        if (y == 0.5f) return sqrtp(x);
+        if (y == 1.f) return x;
+        if (y == 2.f) return x * x;
+        if (y == 4.f) { const float x2 = x * x; return x2 * x2; }
+        return powf(x, y);              /* accurate: the SFU form errs ~1e-5 for |y log2 x| ~ 40 */
+    }
+    static __device__ __forceinline__ R exp(R x) { return expf(x); }
+    static __device__ __forceinline__ R cos_atan(R x) { return rsqrtf(1.f + x * x); }
+    static __device__ __forceinline__ R sin_atan(R x) { return x * rsqrtf(1.f + x * x); }
+    static __device__ __forceinline__ R div(R a, R b) { return __fdividef(a, b); }
+    static __device__ __forceinline__ R qnan() { return __int_as_float(0x7fc00000); }
+    /* settling velocity sqrt(A^2 + c) - A rewritten as c / (sqrt(A^2 + c) + A):
+     * equal in exact arithmetic, but for fine classes (d = 2 um: A = 8.37,
+     * c = 3e-5) the reference's difference cancels ~7 digits, all of FP32's */
+    static __device__ __forceinline__ R settle(R A, R A2, R c) { return __fdividef(c, sqrtp(A2 + c) + A); }
 };
 
 /* hllc of SWEHR.c:327-409 with the velocities already formed
  * (nl = normal/ul, tl = tangential/vl; both 0 for a dry side) and the left
  * side's sqrt(g hl) given.  Same operations as hllc(). */
-__device__ __forceinline__ double hllc_v(double hl, double hr, double nl, double nr, double tl, double tr,
-                                         double g, double cl, double hfilm, double &T0, double &T1, double &T2)
+template <class PP>
+__device__ __forceinline__ typename PP::R hllc_v(typename PP::R hl, typename PP::R hr, typename PP::R nl,
+                                                 typename PP::R nr, typename PP::R tl, typename PP::R tr,
+                                                 typename PP::R g, typename PP::R cl, typename PP::R hfilm,
+                                                 typename PP::R &T0, typename PP::R &T1, typename PP::R &T2)
 {
-    const double cr = sw_sqrt_pow(g * hr);
-    const double d = nl + 2 * cl - nr - 2 * cr;
-    const double hs = (d * d) / (16 * g);
-    const double us = .5 * (nl + nr) + cl - cr;
-    const double cs = sw_sqrt_pow(g * hs);
-    double sl = nl - cl;
+    typedef typename PP::R R;
+    const R half = R(0.5);
+    const R cr = PP::sqrtp(g * hr);
+    const R d = nl + 2 * cl - nr - 2 * cr;
+    const R hs = PP::div(d * d, 16 * g);
+    const R us = half * (nl + nr) + cl - cr;
+    const R cs = PP::sqrtp(g * hs);
+    R sl = nl - cl;
     if (us - cs < sl) sl = us - cs;
-    double sm = us;
-    double sr = nr + cr;
+    R sm = us;
+    R sr = nr + cr;
     if (us + cs > sr) sr = us + cs;
     if (hl <= hfilm) { sl = nr - 2 * cr; sm = sl; sr = nr + cr; }
     if (hr <= hfilm) { sl = nl - cl; sr = nl + 2 * cl; sm = sr; }
-    double f0 = __longlong_as_double(0x7ff8000000000000LL), f1 = f0;
+    R f0 = PP::qnan(), f1 = f0;
     if (sl >= 0) {
         f0 = hl * nl;
-        f1 = hl * nl * nl + .5 * g * hl * hl;
+        f1 = hl * nl * nl + half * g * hl * hl;
     }
     if (sl <= 0 && sr >= 0) {
-        f0 = (sr * (hl * nl) - sl * (hr * nr) + sl * sr * (hr - hl)) / (sr - sl);
-        f1 = (sr * (hl * nl * nl + .5 * g * hl * hl) - sl * (hr * nr * nr + .5 * g * hr * hr)
-              + sl * sr * (hr * nr - hl * nl)) / (sr - sl);
+        f0 = PP::div(sr * (hl * nl) - sl * (hr * nr) + sl * sr * (hr - hl), sr - sl);
+        f1 = PP::div(sr * (hl * nl * nl + half * g * hl * hl) - sl * (hr * nr * nr + half * g * hr * hr)
+                         + sl * sr * (hr * nr - hl * nl),
+                     sr - sl);
     }
     if (sr <= 0) {
         f0 = hr * nr;
-        f1 = hr * nr * nr + .5 * g * hr * hr;
+        f1 = hr * nr * nr + half * g * hr * hr;
     }
     T0 = f0;
     T1 = f1;
     T2 = (sm >= 0) ? f0 * tl : f0 * tr;
-    double s = 0;
+    R s = 0;
     if (fabs(sl) > s) s = fabs(sl);
     if (fabs(sr) > s) s = fabs(sr);
     if (fabs(sm) > s) s = fabs(sm);
@@ -104,22 +138,25 @@ __device__ __forceinline__ double hllc_v(double hl, double hr, double nl, double
 }
 
 /* wave speed only (the same sl, sr, sm as hllc_v) */
-__device__ __forceinline__ double hll_speed(double hl, double hr, double nl, double nr, double g, double cl,
-                                            double hfilm)
+template <class PP>
+__device__ __forceinline__ typename PP::R hll_speed(typename PP::R hl, typename PP::R hr, typename PP::R nl,
+                                                    typename PP::R nr, typename PP::R g, typename PP::R cl,
+                                                    typename PP::R hfilm)
 {
-    const double cr = sw_sqrt_pow(g * hr);
-    const double d = nl + 2 * cl - nr - 2 * cr;
-    const double hs = (d * d) / (16 * g);
-    const double us = .5 * (nl + nr) + cl - cr;
-    const double cs = sw_sqrt_pow(g * hs);
-    double sl = nl - cl;
+    typedef typename PP::R R;
+    const R cr = PP::sqrtp(g * hr);
+    const R d = nl + 2 * cl - nr - 2 * cr;
+    const R hs = PP::div(d * d, 16 * g);
+    const R us = R(0.5) * (nl + nr) + cl - cr;
+    const R cs = PP::sqrtp(g * hs);
+    R sl = nl - cl;
     if (us - cs < sl) sl = us - cs;
-    double sm = us;
-    double sr = nr + cr;
+    R sm = us;
+    R sr = nr + cr;
     if (us + cs > sr) sr = us + cs;
     if (hl <= hfilm) { sl = nr - 2 * cr; sm = sl; sr = nr + cr; }
     if (hr <= hfilm) { sl = nl - cl; sr = nl + 2 * cl; sm = sr; }
-    double s = 0;
+    R s = 0;
     if (fabs(sl) > s) s = fabs(sl);
     if (fabs(sr) > s) s = fabs(sr);
     if (fabs(sm) > s) s = fabs(sm);
@@ -139,92 +176,271 @@ __device__ __forceinline__ TileCoord tile_coord(const DevParams &P, int64_t tile
     return t;
 }
 
-/* Stage A: halo cells of the tile.  what: 0 = wave pass (h u v g c),
- * 1 = update pass (+ SED_k, TOTSED, DEP). */
-template <int WHAT>
-__device__ __forceinline__ void stage_halo(const DevParams &P, const double *__restrict__ src,
-                                           const double *__restrict__ zp, TileCoord tc, double *sm,
-                                           const TileLayout &TL, double inh, double inhv, double insed)
+/* -------------------------------------------------------------- staging ---
+ * Every global load of a tile is issued up front as an asynchronous copy
+ * (cp.async, 2 elements per copy) into shared memory, so the arithmetic never
+ * waits on HBM and other CTAs on the SM compute while this one's copies fly.
+ *   halo planes  h hu hv totsed dep U_1..U_S   10 rows x 36 columns
+ *   cell planes  totm maxvel maxdep [ks] (RS), vinf M_1..M_S (double)   8 x 32
+ *   topography   z_prev 12 x 36, z 10 x 36
+ * Row r of a halo plane is grid row i0-1+r; column c is grid column
+ * (0-based) j0-3+c, so halo cell (hi, hj) sits at (hi, hj+1) and the first
+ * column is 16-byte aligned.  Rows or columns outside the grid are not
+ * loaded: ghosts are resolved from their source cells afterwards
+ * (SWEHR.c:816-1035). */
+#define R_J 36              /* staged columns */
+#define HALO_ROWS H_I       /* 10 */
+#define ZP_ROWS 12
+#define ZC_ROWS 10
+
+struct StagedLayout {
+    /* byte offsets from the start of dynamic shared memory */
+    size_t halo, cell_r, cell_d, zp, zc, u, v, g, c, sed, fx, fy, up, red, total;
+    int nhalo, ncellr, ncelld;
+    __host__ __device__ static StagedLayout make(int S, size_t rs, int what)
+    {
+        StagedLayout L;
+        size_t o = 0;
+        auto take = [&](size_t bytes) { size_t at = o; o += (bytes + 15) / 16 * 16; return at; };
+        L.nhalo = what ? 5 + S : 3;
+        L.ncellr = what ? 4 : 0;
+        L.ncelld = what ? 1 + S : 0;
+        L.halo = take((size_t)L.nhalo * HALO_ROWS * R_J * rs);
+        L.cell_r = take((size_t)L.ncellr * T_I * T_J * rs);
+        L.cell_d = take((size_t)L.ncelld * T_I * T_J * sizeof(double));
+        L.zp = take((size_t)ZP_ROWS * R_J * sizeof(double));
+        L.zc = take(what ? (size_t)ZC_ROWS * R_J * sizeof(double) : 0);
+        L.u = take((size_t)N_H * rs);
+        L.v = take((size_t)N_H * rs);
+        L.g = take((size_t)N_H * rs);
+        L.c = take((size_t)N_H * rs);
+        L.sed = take(what ? (size_t)S * N_H * rs : 0);
+        L.fx = take(what ? (size_t)3 * N_FX * rs : 0);
+        L.fy = take(what ? (size_t)3 * N_FY * rs : 0);
+        L.up = take(what ? (size_t)(N_FX + N_FY) : 0);
+        L.red = take(what ? (size_t)(TILE_THREADS / 32) * B_NTERMS * sizeof(double) : 0);
+        L.total = o;
+        return L;
+    }
+};
+
+/* halo planes, in staging order */
+enum { HP_H = 0, HP_HU, HP_HV, HP_TS, HP_DEP, HP_U };
+/* cell planes: RS then double */
+enum { CR_TOTM = 0, CR_MAXVEL, CR_MAXDEP, CR_KS };
+enum { CD_VINF = 0, CD_M };
+
+template <class RS>
+__device__ __forceinline__ const RS *halo_plane_src(const SetV<RS> &s, int p, int64_t pl)
+{
+    switch (p) {
+    case HP_H: return s.h;
+    case HP_HU: return s.hu;
+    case HP_HV: return s.hv;
+    case HP_TS: return s.totsed;
+    case HP_DEP: return s.dep;
+    default: return s.U + (int64_t)(p - HP_U) * pl;
+    }
+}
+
+/* pair copy global -> shared: 2 elements of T (8 or 16 bytes) */
+template <class T>
+__device__ __forceinline__ void cp_pair(void *dst, const T *src)
+{
+    __pipeline_memcpy_async(dst, src, 2 * sizeof(T));
+}
+
+/* Issue the tile's asynchronous copies.  WHAT = 0: wave pass (h hu hv, z_prev);
+ * 1: update pass (all). */
+template <class RS, int WHAT>
+__device__ __forceinline__ void stage_load(const DevParams &P, const SetV<RS> &src, const double *__restrict__ zp,
+                                           const double *__restrict__ zc, const RS *__restrict__ ks, TileCoord tc,
+                                           unsigned char *smb, const StagedLayout &L)
 {
     const int64_t pl = P.plane;
+    const int c0 = tc.j0 - 3;                                  /* 0-based grid column of staged column 0 */
+    /* halo planes: 10 rows x 18 pairs per plane */
+    RS *halo = reinterpret_cast<RS *>(smb + L.halo);
+    for (int job = threadIdx.x; job < L.nhalo * HALO_ROWS * (R_J / 2); job += TILE_THREADS) {
+        const int p = job / (HALO_ROWS * (R_J / 2));
+        const int rem = job - p * (HALO_ROWS * (R_J / 2));
+        const int r = rem / (R_J / 2), k2 = rem - r * (R_J / 2);
+        const int gi = tc.i0 - 1 + r, col = c0 + 2 * k2;
+        if (gi < 1 || gi > P.nx || col < 0 || col >= P.pitch) continue;
+        cp_pair(halo + (p * HALO_ROWS + r) * R_J + 2 * k2, halo_plane_src(src, p, pl) + (int64_t)(gi - 1) * P.pitch + col);
+    }
+    /* topography: z_prev rows i0-2.., z rows i0-1.. */
+    double *zps = reinterpret_cast<double *>(smb + L.zp);
+    double *zcs = reinterpret_cast<double *>(smb + L.zc);
+    const int nz = (ZP_ROWS + (WHAT ? ZC_ROWS : 0)) * (R_J / 2);
+    for (int job = threadIdx.x; job < nz; job += TILE_THREADS) {
+        const bool isp = job < ZP_ROWS * (R_J / 2);
+        const int j2 = isp ? job : job - ZP_ROWS * (R_J / 2);
+        const int r = j2 / (R_J / 2), k2 = j2 - r * (R_J / 2);
+        const int gi = (isp ? tc.i0 - 2 : tc.i0 - 1) + r, col = c0 + 2 * k2;
+        if (gi < 1 || gi > P.nx || col < 0 || col >= P.pitch) continue;
+        cp_pair((isp ? zps : zcs) + r * R_J + 2 * k2, (isp ? zp : zc) + (int64_t)(gi - 1) * P.pitch + col);
+    }
+    if (WHAT) {
+        /* cell planes: 8 rows x 16 pairs */
+        RS *cr = reinterpret_cast<RS *>(smb + L.cell_r);
+        double *cd = reinterpret_cast<double *>(smb + L.cell_d);
+        const int nr = (P.has_ks ? 4 : 3), njob = (nr + L.ncelld) * T_I * (T_J / 2);
+        for (int job = threadIdx.x; job < njob; job += TILE_THREADS) {
+            const int p = job / (T_I * (T_J / 2));
+            const int rem = job - p * (T_I * (T_J / 2));
+            const int r = rem / (T_J / 2), k2 = rem - r * (T_J / 2);
+            const int gi = tc.i0 + r, col = tc.j0 - 1 + 2 * k2;
+            if (gi > P.nx || col >= P.pitch) continue;
+            const int64_t go = (int64_t)(gi - 1) * P.pitch + col;
+            if (p < nr) {
+                const RS *sp = p == CR_TOTM ? src.totm : p == CR_MAXVEL ? src.maxvel : p == CR_MAXDEP ? src.maxdep : ks;
+                cp_pair(cr + (p * T_I + r) * T_J + 2 * k2, sp + go);
+            } else {
+                const int d = p - nr;
+                const double *sp = d == CD_VINF ? src.vinf : src.M + (int64_t)(d - CD_M) * pl;
+                cp_pair(cd + (d * T_I + r) * T_J + 2 * k2, sp + go);
+            }
+        }
+    }
+    __pipeline_commit();
+}
+
+/* slopes from a staged topography tile, same operations as slope_x/slope_y
+ * (SWEHR.c:1240-1277); (r, c) is the staged position of grid cell (i, j) */
+__device__ __forceinline__ double sslope_x(const DevParams &P, const double *zs, int r, int c, int i)
+{
+    if (i != 1 && i != P.nx) return P.half_odx * (zs[(r + 1) * R_J + c] - zs[(r - 1) * R_J + c]);
+    if (i == P.nx) return P.oneoverdx * (zs[r * R_J + c] - zs[(r - 1) * R_J + c]);
+    return P.oneoverdx * (zs[(r + 1) * R_J + c] - zs[r * R_J + c]);
+}
+
+__device__ __forceinline__ double sslope_y(const DevParams &P, const double *zs, int r, int c, int j)
+{
+    if (j != 1 && j != P.ny) return P.half_odx * (zs[r * R_J + c + 1] - zs[r * R_J + c - 1]);
+    if (j == P.ny) return P.oneoverdx * (zs[r * R_J + c] - zs[r * R_J + c - 1]);
+    return P.oneoverdx * (zs[r * R_J + c + 1] - zs[r * R_J + c]);
+}
+
+/* Derived halo values from the staged planes: h, u = hu/h, v = hv/h (0 when
+ * dry), GZ of the previous step and sqrt(GZ h) for left/lower face cells,
+ * SED_k.  Ghost cells read their source cell (SWEHR.c:816-1035). */
+template <class PP, class RS, int WHAT>
+__device__ __forceinline__ void stage_derive(const DevParams &P, TileCoord tc, unsigned char *smb,
+                                             const StagedLayout &L, typename PP::R inh, typename PP::R inhv,
+                                             typename PP::R insed)
+{
+    typedef typename PP::R R;
+    const RealC<R> &K = kc<R>(P);
+    const RS *halo = reinterpret_cast<const RS *>(smb + L.halo);
+    const double *zps = reinterpret_cast<const double *>(smb + L.zp);
+    R *su = reinterpret_cast<R *>(smb + L.u), *sv = reinterpret_cast<R *>(smb + L.v);
+    R *sg = reinterpret_cast<R *>(smb + L.g), *sc = reinterpret_cast<R *>(smb + L.c);
+    R *ssed = reinterpret_cast<R *>(smb + L.sed);
     for (int idx = threadIdx.x; idx < N_H; idx += TILE_THREADS) {
-        const int hi = idx / H_J, hj = idx % H_J;
+        const int hi = idx / H_J, hj = idx - hi * H_J;
         const int gi = tc.i0 - 1 + hi, gj = tc.j0 - 1 + hj;
         const bool hcorner = (hi == 0 || hi == H_I - 1) && (hj == 0 || hj == H_J - 1);
         const bool gx = gi == 0 || gi == P.nx + 1, gy = gj == 0 || gj == P.ny + 1;
         if (hcorner || gi > P.nx + 1 || gj > P.ny + 1 || (gx && gy)) continue;
         const int si = gi < 1 ? 1 : (gi > P.nx ? P.nx : gi);
         const int sj = gj < 1 ? 1 : (gj > P.ny ? P.ny : gj);
+        const int sr = si - (tc.i0 - 1), scol = sj - (tc.j0 - 2);          /* staged position of the source */
+        const int so = sr * R_J + scol;
         const bool inflow = gj == P.ny + 1 && P.inflow;
-        double h, hu, hv;
-        const int64_t q = cidx(P, si, sj);
+        R h, hu, hv;
         if (inflow) {
             h = inh; hu = 0; hv = inhv;
         } else {
-            h = src[P_H * pl + q];
-            hu = src[P_HU * pl + q];
-            hv = src[P_HV * pl + q];
+            h = (R)halo[(HP_H * HALO_ROWS) * R_J + so];
+            hu = (R)halo[(HP_HU * HALO_ROWS) * R_J + so];
+            hv = (R)halo[(HP_HV * HALO_ROWS) * R_J + so];
             if ((gi == 0 && P.bndry[0] == 1) || (gi == P.nx + 1 && P.bndry[2] == 1)) hu = -hu;
             if ((gj == 0 && P.bndry[1] == 1) || (gj == P.ny + 1 && P.bndry[3] == 1)) hv = -hv;
         }
-        double u = 0, v = 0;
-        if (h > P.hfilm) { u = hu / h; v = hv / h; }
-        sm[TL.h + idx] = h;
-        sm[TL.u + idx] = u;
-        sm[TL.v + idx] = v;
+        R u = 0, v = 0;
+        if (h > K.hfilm) { u = PP::div(hu, h); v = PP::div(hv, h); }
+        if (gx || gy) {
+            /* ghost cells are never read through the staged planes: keep h there */
+            reinterpret_cast<RS *>(smb + L.halo)[(HP_H * HALO_ROWS + hi) * R_J + hj + 1] = (RS)h;
+        }
+        su[idx] = u;
+        sv[idx] = v;
         if (hi <= T_I && hj <= T_J) {
-            const double g = gz_of(P, zp, si, sj);
-            sm[TL.g + idx] = g;
-            sm[TL.c + idx] = sw_sqrt_pow(g * h);
+            /* GZ of the previous step at the source cell, SWEHR.c:1279 via z_prev */
+            const int zr = si - (tc.i0 - 2);
+            const R sx = (R)sslope_x(P, zps, zr, scol, si), sy = (R)sslope_y(P, zps, zr, scol, sj);
+            const R g = PP::div(K.g, PP::sqrtp(sx * sx + sy * sy + 1));
+            sg[idx] = g;
+            sc[idx] = PP::sqrtp(g * h);
         }
         if (WHAT == 1) {
-            for (int k = 0; k < P.S; k++)
-                sm[TL.sed + k * N_H + idx] = inflow ? insed : sed_of(src[(P_FIXED + k) * pl + q], h, P.hfilm);
-            if (!gx && !gy) {
-                sm[TL.ts + idx] = src[P_TOTSED * pl + q];
-                sm[TL.dep + idx] = src[P_DEP * pl + q];
+            for (int k = 0; k < P.S; k++) {
+                R s = 0;
+                if (inflow) s = insed;
+                else if (h > K.hfilm) {
+                    s = PP::div((R)halo[((HP_U + k) * HALO_ROWS) * R_J + so], h);
+                    if (s < R(-1e-5)) s = 0;
+                }
+                ssed[k * N_H + idx] = s;
             }
         }
     }
 }
 
-/* ------------------------------------------------------------------ wave */
-__global__ void __launch_bounds__(TILE_THREADS) k_wave_tile(const DevParams P, const Bufs B, Ctl *ctl)
+/* halo-cell depth as staged (ghosts filled by stage_derive) */
+template <class RS>
+__device__ __forceinline__ const RS *staged_h(const unsigned char *smb, const StagedLayout &L)
 {
+    return reinterpret_cast<const RS *>(smb + L.halo) + (HP_H * HALO_ROWS) * R_J;
+}
+
+/* ------------------------------------------------------------------ wave */
+template <class PP, class RS>
+__global__ void __launch_bounds__(TILE_THREADS) k_wave_tile(const DevParams P, const BufsT<RS> B, Ctl *ctl)
+{
+    typedef typename PP::R R;
     if (!ctl->active) return;
-    extern __shared__ double sm[];
-    const TileLayout TL = TileLayout::make(0);
+    extern __shared__ __align__(16) unsigned char smb[];
+    const StagedLayout L = StagedLayout::make(0, sizeof(R), 0);
+    const RealC<R> &K = kc<R>(P);
     const int64_t n = ctl->step;
     const double t = ctl->t;
-    const double *src = B.set[n & 1];
+    const SetV<RS> src = B.set[n & 1];
     const double *zp = B.z[(n + 2) % 3];
     double inh = 0, inhv = 0, insed = 0;
     if (P.inflow) inflow_ghost(t, inh, inhv, insed);
     const int64_t ntiles = (int64_t)((P.nx + T_I - 1) / T_I) * ((P.ny + T_J - 1) / T_J);
-    double smax = 0;
+    const R *su = reinterpret_cast<const R *>(smb + L.u), *sv = reinterpret_cast<const R *>(smb + L.v);
+    const R *sg = reinterpret_cast<const R *>(smb + L.g), *sc = reinterpret_cast<const R *>(smb + L.c);
+    R smax = 0;
     for (int64_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
         const TileCoord tc = tile_coord(P, tile);
-        stage_halo<0>(P, src, zp, tc, sm, TL, inh, inhv, insed);
+        stage_load<RS, 0>(P, src, zp, nullptr, nullptr, tc, smb, L);
+        __pipeline_wait_prior(0);
         __syncthreads();
+        stage_derive<PP, RS, 0>(P, tc, smb, L, (R)inh, (R)inhv, (R)insed);
+        __syncthreads();
+        const RS *sh = staged_h<RS>(smb, L);
         /* faces owned by the tile: i+1/2 and j+1/2 of its cells, plus the
          * domain's low boundary faces 1/2 */
         for (int f = threadIdx.x; f < N_FX + N_FY; f += TILE_THREADS) {
             if (f < N_FX) {
-                const int fi = f / T_J, fj = f % T_J;
+                const int fi = f / T_J, fj = f - fi * T_J;
                 const int gi = tc.i0 - 1 + fi, gj = tc.j0 + fj;
                 if (gj > P.ny || gi > P.nx || (fi == 0 && gi != 0)) continue;
-                const int L = fi * H_J + fj + 1, R = L + H_J;
-                const double s = hll_speed(sm[TL.h + L], sm[TL.h + R], sm[TL.u + L], sm[TL.u + R], sm[TL.g + L],
-                                           sm[TL.c + L], P.hfilm);
+                const int Lh = fi * H_J + fj + 1, Rh = Lh + H_J;
+                const R s = hll_speed<PP>((R)sh[fi * R_J + fj + 2], (R)sh[(fi + 1) * R_J + fj + 2], su[Lh], su[Rh],
+                                          sg[Lh], sc[Lh], K.hfilm);
                 smax = (s > smax) ? s : smax;
             } else {
                 const int f2 = f - N_FX;
-                const int fi = f2 / (T_J + 1), fj = f2 % (T_J + 1);
+                const int fi = f2 / (T_J + 1), fj = f2 - fi * (T_J + 1);
                 const int gi = tc.i0 + fi, gj = tc.j0 - 1 + fj;
                 if (gi > P.nx || gj > P.ny || (fj == 0 && gj != 0)) continue;
-                const int L = (fi + 1) * H_J + fj, R = L + 1;
-                const double s = hll_speed(sm[TL.h + L], sm[TL.h + R], sm[TL.v + L], sm[TL.v + R], sm[TL.g + L],
-                                           sm[TL.c + L], P.hfilm);
+                const int Lh = (fi + 1) * H_J + fj, Rh = Lh + 1;
+                const R s = hll_speed<PP>((R)sh[(fi + 1) * R_J + fj + 1], (R)sh[(fi + 1) * R_J + fj + 2], sv[Lh],
+                                          sv[Rh], sg[Lh], sc[Lh], K.hfilm);
                 smax = (s > smax) ? s : smax;
             }
         }
@@ -232,8 +448,8 @@ __global__ void __launch_bounds__(TILE_THREADS) k_wave_tile(const DevParams P, c
     }
     __shared__ double red[TILE_THREADS / 32];
     __shared__ bool last;
-    smax = warp_max(smax);
-    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = smax;
+    double smd = warp_max((double)smax);
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = smd;
     __syncthreads();
     if (threadIdx.x == 0) {
         double m = 0;
@@ -259,12 +475,11 @@ __global__ void __launch_bounds__(TILE_THREADS) k_wave_tile(const DevParams P, c
     ctl->wave_ticket = 0u;
     ctl->pending = 1;
 }
-
 /* ---------------------------------------------------------------- update */
 template <int MAXS, bool BUDGET>
 struct Acc2 {
-    double rain, out, clamp, bulk, inf;
-    double det[BUDGET ? MAXS : 1], sout[BUDGET ? MAXS : 1];
+    double rain, out, clamp, bulk, inf, round;
+    double det[BUDGET ? MAXS : 1], sout[BUDGET ? MAXS : 1], sround[BUDGET ? MAXS : 1];
 };
 
 /* Parameters of the exact slope-failure test (passed by value: a pointer to
@@ -292,67 +507,91 @@ __device__ __forceinline__ double fa_slope_y(const FailArgs &A, const double *__
     return A.oneoverdx * (z[q + 1] - z[q]);
 }
 
-/* Exact slope-failure test, SWEHR.c:1292-1312 (rarely needed). */
-__device__ __noinline__ double fail_exact(const FailArgs A, const double *__restrict__ dep_plane,
-                                          const double *__restrict__ zp, const double *__restrict__ zc, int i, int j,
-                                          double sx, double sy, double gz, double dep0, double rho0c, double h0v)
+/* Exact slope-failure test, SWEHR.c:1292-1312, in the form's arithmetic
+ * (rarely needed: see the bound in tile_cell). */
+template <class PP, class RS>
+__device__ __noinline__ typename PP::R fail_exact(const FailArgs A, const RS *__restrict__ dep_plane,
+                                                  const double *__restrict__ zp, const double *__restrict__ zc,
+                                                  int i, int j, typename PP::R sx, typename PP::R sy,
+                                                  typename PP::R gz, typename PP::R dep0, typename PP::R rho0c,
+                                                  typename PP::R h0v)
 {
+    typedef typename PP::R R;
     const int iu = (i < A.nx) ? i + 1 : A.nx, id = (i > 1) ? i - 1 : 1;
     const int ju = (j < A.ny) ? j + 1 : A.ny, jd = (j > 1) ? j - 1 : 1;
-    const double sxu = (iu == i) ? sx : fa_slope_x(A, zp, iu, j);
-    const double sxd = (id == i) ? sx : fa_slope_x(A, zc, id, j);
-    const double syu = (ju == j) ? sy : fa_slope_y(A, zp, i, ju);
-    const double syd = (jd == j) ? sy : fa_slope_y(A, zc, i, jd);
-    const double rho0 = A.rho0;
-    auto D = [&](int ii, int jj) { return dep_plane[(int64_t)(ii - 1) * A.pitch + (jj - 1)]; };
-    double fail = 0;
-    double pgfx = dep0 * rho0 * gz * 0.5 * A.oneoverdx
-                  * (D(iu, j) * sw_cos_atan(fabs(sxu)) - D(id, j) * sw_cos_atan(fabs(sxd)));
+    const R sxu = (iu == i) ? sx : (R)fa_slope_x(A, zp, iu, j);
+    const R sxd = (id == i) ? sx : (R)fa_slope_x(A, zc, id, j);
+    const R syu = (ju == j) ? sy : (R)fa_slope_y(A, zp, i, ju);
+    const R syd = (jd == j) ? sy : (R)fa_slope_y(A, zc, i, jd);
+    const R rho0 = (R)A.rho0, half = R(0.5), odx = (R)A.oneoverdx;
+    auto D = [&](int ii, int jj) { return (R)dep_plane[(int64_t)(ii - 1) * A.pitch + (jj - 1)]; };
+    R fail = 0;
+    R pgfx = dep0 * rho0 * gz * half * odx
+             * (D(iu, j) * PP::cos_atan(fabs(sxu)) - D(id, j) * PP::cos_atan(fabs(sxd)));
     if (pgfx * sx > 0) pgfx = -1 * fabs(pgfx);
     if (pgfx * sx < 0) pgfx = fabs(pgfx);
-    const double lhs = (rho0 * gz * dep0 + rho0c * gz * h0v) * sw_sin_atan(fabs(sy));
-    const double nrm = (rho0 * gz * dep0 + rho0c * gz * h0v) * sw_cos_atan(fabs(sy)) - A.rhow * gz * (dep0 + h0v);
-    if (fail == 0 && (lhs > (A.cohesion + nrm * A.fa + pgfx))) fail = 1;
-    double pgfy = dep0 * rho0 * gz * 0.5 * A.oneoverdx
-                  * (D(i, ju) * sw_cos_atan(fabs(syu)) - D(i, jd) * sw_cos_atan(fabs(syd)));
+    const R lhs = (rho0 * gz * dep0 + rho0c * gz * h0v) * PP::sin_atan(fabs(sy));
+    const R nrm = (rho0 * gz * dep0 + rho0c * gz * h0v) * PP::cos_atan(fabs(sy)) - (R)A.rhow * gz * (dep0 + h0v);
+    if (fail == 0 && (lhs > ((R)A.cohesion + nrm * (R)A.fa + pgfx))) fail = 1;
+    R pgfy = dep0 * rho0 * gz * half * odx
+             * (D(i, ju) * PP::cos_atan(fabs(syu)) - D(i, jd) * PP::cos_atan(fabs(syd)));
     if (pgfy * sy > 0) pgfy = -1 * fabs(pgfy);
     if (pgfy * sy < 0) pgfy = fabs(pgfy);
-    if (fail == 0 && (lhs > (A.cohesion + nrm * A.fa + pgfy))) fail = 1;
+    if (fail == 0 && (lhs > ((R)A.cohesion + nrm * (R)A.fa + pgfy))) fail = 1;
     return fail;
 }
 
-template <int MAXS, bool BUDGET>
-__device__ __forceinline__ void tile_cell(const DevParams &P, const double *__restrict__ src, double *__restrict__ dst,
-                                          const double *__restrict__ zp, const double *__restrict__ zc,
-                                          double *__restrict__ zn, const double *__restrict__ ksf, const double *sm,
-                                          const TileLayout &TL, TileCoord tc, double t, double dt, double Rr,
-                                          Acc2<MAXS, BUDGET> &acc)
+/* moving storm in the form's arithmetic (positions in FP64) */
+template <class PP>
+__device__ __forceinline__ typename PP::R storm_r(const DevParams &P, double t, int i, int j)
 {
+    typedef typename PP::R R;
+    const double x = ((double)i - 0.5) * P.dx - (P.storm_x0 + P.storm_vx * t);
+    const double y = ((double)j - 0.5) * P.dx - (P.storm_y0 + P.storm_vy * t);
+    const double r2 = (x * x + y * y) / P.storm_r2;
+    return (R)P.storm_peak * PP::exp(R(-0.5 * r2));
+}
+
+template <class PP, class RS, int MAXS, bool BUDGET>
+__device__ __forceinline__ void tile_cell(const DevParams &P, const SetV<RS> &src, const SetV<RS> &dst,
+                                          const double *__restrict__ zp, const double *__restrict__ zc,
+                                          double *__restrict__ zn, const unsigned char *smb, const StagedLayout &L,
+                                          TileCoord tc, double t, double dt, double Rr, Acc2<MAXS, BUDGET> &acc)
+{
+    typedef typename PP::R R;
+    const RealC<R> &K = kc<R>(P);
     const int ti = threadIdx.x / T_J, tj = threadIdx.x % T_J;
     const int i = tc.i0 + ti, j = tc.j0 + tj;
     if (i > P.nx || j > P.ny) return;
     const int64_t pl = P.plane;
     const int64_t q = cidx(P, i, j);
     const int S = P.S;
-    const double hfilm = P.hfilm, rhos = P.rhos, rhow = P.rhow;
+    const R hfilm = K.hfilm, rhos = K.rhos, rhow = K.rhow, one = 1, half = R(0.5);
     const int hs = (ti + 1) * H_J + (tj + 1);                      /* this cell in halo coords */
-    const double h0v = sm[TL.h + hs];
-    const double hu0 = src[P_HU * pl + q], hv0 = src[P_HV * pl + q];
-    const double totsed0 = sm[TL.ts + hs], dep0 = sm[TL.dep + hs];
-    const double totm0 = src[P_TOTM * pl + q];
-    double rho0c = rhow * (1 - totsed0) + rhos * totsed0;
-    if (rho0c > P.rhos08) rho0c = P.rhos08;
-    const double Rc = P.storm ? storm_at(P, t, i, j) : Rr;
+    const int so = (ti + 1) * R_J + (tj + 2);                      /* ... and in the staged planes */
+    const int cs = ti * T_J + tj;                                  /* ... and in the cell planes */
+    const RS *halo = reinterpret_cast<const RS *>(smb + L.halo);
+    const RS *cellr = reinterpret_cast<const RS *>(smb + L.cell_r);
+    const double *celld = reinterpret_cast<const double *>(smb + L.cell_d);
+    const RS *sTS = halo + (HP_TS * HALO_ROWS) * R_J, *sDEP = halo + (HP_DEP * HALO_ROWS) * R_J;
+    const R h0v = (R)halo[(HP_H * HALO_ROWS) * R_J + so];
+    const R hu0 = (R)halo[(HP_HU * HALO_ROWS) * R_J + so], hv0 = (R)halo[(HP_HV * HALO_ROWS) * R_J + so];
+    const R totsed0 = (R)sTS[so], dep0 = (R)sDEP[so];
+    const R totm0 = (R)cellr[CR_TOTM * T_I * T_J + cs];
+    R rho0c = rhow * (1 - totsed0) + rhos * totsed0;
+    if (rho0c > K.rhos08) rho0c = K.rhos08;
+    const R Rc = P.storm ? storm_r<PP>(P, t, i, j) : (R)Rr;
+    const R dtr = (R)dt;
 
     /* faces of this cell (computed in stage B) */
     const int fxl = ti * T_J + tj, fxr = (ti + 1) * T_J + tj;
     const int fyl = ti * (T_J + 1) + tj, fyr = fyl + 1;
-    const unsigned char *up = reinterpret_cast<const unsigned char *>(sm + TL.up);
-    const double *FX = sm + TL.fx, *FY = sm + TL.fy;
-    const double fxl0 = FX[3 * fxl], fxl1 = FX[3 * fxl + 1], fxl2 = FX[3 * fxl + 2];
-    const double fxr0 = FX[3 * fxr], fxr1 = FX[3 * fxr + 1], fxr2 = FX[3 * fxr + 2];
-    const double fyl0 = FY[3 * fyl], fyl1 = FY[3 * fyl + 1], fyl2 = FY[3 * fyl + 2];
-    const double fyr0 = FY[3 * fyr], fyr1 = FY[3 * fyr + 1], fyr2 = FY[3 * fyr + 2];
+    const R *FX = reinterpret_cast<const R *>(smb + L.fx), *FY = reinterpret_cast<const R *>(smb + L.fy);
+    const unsigned char *up = smb + L.up;
+    const R fxl0 = FX[3 * fxl], fxl1 = FX[3 * fxl + 1], fxl2 = FX[3 * fxl + 2];
+    const R fxr0 = FX[3 * fxr], fxr1 = FX[3 * fxr + 1], fxr2 = FX[3 * fxr + 2];
+    const R fyl0 = FY[3 * fyl], fyl1 = FY[3 * fyl + 1], fyl2 = FY[3 * fyl + 2];
+    const R fyr0 = FY[3 * fyr], fyr1 = FY[3 * fyr + 1], fyr2 = FY[3 * fyr + 2];
     /* upwind cells of the sediment fluxes, halo index */
     const int uxl = up[fxl] ? hs : hs - H_J;
     const int uxr = up[fxr] ? hs + H_J : hs;
@@ -360,162 +599,178 @@ __device__ __forceinline__ void tile_cell(const DevParams &P, const double *__re
     const int uyr = up[N_FX + fyr] ? hs + 1 : hs;
 
     /* sources, SWEHR.c:1239-1320 */
-    const double g = P.g;
-    const double sx = slope_x(P, zc, i, j), sy = slope_y(P, zc, i, j);
-    const double syl = slope_y(P, zp, i, j);
-    const double gx = g * sx / sw_sqrt_pow(sx * sx + syl * syl + 1);
-    const double SXf = -gx * h0v;
-    const double gy = g * sy / sw_sqrt_pow(sx * sx + sy * sy + 1);
-    const double SYf = -gy * h0v;
-    const double gz = g / sw_sqrt_pow(sx * sx + sy * sy + 1);
-    const double slope = sw_sqrt_pow(sx * sx + sy * sy);
-    double gammax = 0, gammay = 0;
+    const R g = K.g;
+    const double *zps = reinterpret_cast<const double *>(smb + L.zp), *zcs = reinterpret_cast<const double *>(smb + L.zc);
+    const R sx = (R)sslope_x(P, zcs, ti + 1, tj + 2, i), sy = (R)sslope_y(P, zcs, ti + 1, tj + 2, j);
+    const R syl = (R)sslope_y(P, zps, ti + 2, tj + 2, j);
+    const R gx = PP::div(g * sx, PP::sqrtp(sx * sx + syl * syl + 1));
+    const R SXf = -gx * h0v;
+    const R gy = PP::div(g * sy, PP::sqrtp(sx * sx + sy * sy + 1));
+    const R SYf = -gy * h0v;
+    const R gz = PP::div(g, PP::sqrtp(sx * sx + sy * sy + 1));
+    const R slope = PP::sqrtp(sx * sx + sy * sy);
+    R gammax = 0, gammay = 0;
     if (i > 1 && i < P.nx)
-        gammax -= (rhos - rho0c) * gz * h0v * h0v / (2 * rho0c) * .5 * P.oneoverdx
-                  * (sm[TL.ts + hs + H_J] - sm[TL.ts + hs - H_J]);
+        gammax -= PP::div((rhos - rho0c) * gz * h0v * h0v, 2 * rho0c) * half * K.oneoverdx
+                  * ((R)sTS[so + R_J] - (R)sTS[so - R_J]);
     if (j > 1 && j < P.ny)
-        gammay -= (rhos - rho0c) * gz * h0v * h0v / (2 * rho0c) * .5 * P.oneoverdx
-                  * (sm[TL.ts + hs + 1] - sm[TL.ts + hs - 1]);
+        gammay -= PP::div((rhos - rho0c) * gz * h0v * h0v, 2 * rho0c) * half * K.oneoverdx
+                  * ((R)sTS[so + 1] - (R)sTS[so - 1]);
     /* slope stability: provable "no failure" first, exact test otherwise */
-    double fail = 0;
+    R fail = 0;
     {
-        const double rho0 = P.rho0;
-        const double A = rho0 * gz * dep0 + rho0c * gz * h0v;
-        const double s = fabs(sy);
-        const double depx = fabs(sm[TL.dep + (i < P.nx ? hs + H_J : hs)]) + fabs(sm[TL.dep + (i > 1 ? hs - H_J : hs)]);
-        const double depy = fabs(sm[TL.dep + (j < P.ny ? hs + 1 : hs)]) + fabs(sm[TL.dep + (j > 1 ? hs - 1 : hs)]);
-        const double pb = fabs(dep0) * rho0 * fabs(gz) * 0.5 * P.oneoverdx * fmax(depx, depy);
-        const double w = P.rhow * gz * (dep0 + h0v);
-        const double lhs_ub = A * s;
-        const double rhs_lb = P.cohesion + (A * (1 - 0.5 * s * s) - w) * P.fa - pb;
-        const double margin = 1e-6 * (fabs(A) * (1 + s) + P.cohesion + fabs(w) * P.fa + pb) + 1e-300;
-        const bool safe = A >= 0 && gz > 0 && P.fa >= 0 && lhs_ub + margin < rhs_lb;
+        const R rho0 = K.rho0;
+        const R A = rho0 * gz * dep0 + rho0c * gz * h0v;
+        const R s = fabs(sy);
+        const R depx = fabs((R)sDEP[i < P.nx ? so + R_J : so]) + fabs((R)sDEP[i > 1 ? so - R_J : so]);
+        const R depy = fabs((R)sDEP[j < P.ny ? so + 1 : so]) + fabs((R)sDEP[j > 1 ? so - 1 : so]);
+        const R pb = fabs(dep0) * rho0 * fabs(gz) * half * K.oneoverdx * fmax(depx, depy);
+        const R w = rhow * gz * (dep0 + h0v);
+        const R lhs_ub = A * s;
+        const R rhs_lb = K.cohesion + (A * (1 - half * s * s) - w) * K.fa - pb;
+        const R margin = R(1e-5) * (fabs(A) * (1 + s) + K.cohesion + fabs(w) * K.fa + pb) + R(1e-30);
+        const bool safe = A >= 0 && gz > 0 && K.fa >= 0 && lhs_ub + margin < rhs_lb;
         if (!safe) {
             FailArgs fa;
             fa.nx = P.nx; fa.ny = P.ny; fa.pitch = P.pitch; fa.pad_ = 0; fa.plane = P.plane;
             fa.oneoverdx = P.oneoverdx; fa.half_odx = P.half_odx; fa.rho0 = P.rho0; fa.rhow = P.rhow;
             fa.cohesion = P.cohesion; fa.fa = P.fa;
-            fail = fail_exact(fa, src + P_DEP * pl, zp, zc, i, j, sx, sy, gz, dep0, rho0c, h0v);
+            fail = fail_exact<PP, RS>(fa, src.dep, zp, zc, i, j, sx, sy, gz, dep0, rho0c, h0v);
         }
     }
-    double dfmask = fmin(1.0, (totsed0 - 0.2) / 0.2);
-    if (h0v < P.h0x9 || totsed0 < 0.2) dfmask = 0;
-    double betax = P.neg1ml * gz * h0v * P.fa;
-    double betay = P.neg1ml * gz * h0v * P.fa;
+    R dfmask = fmin(one, PP::div(totsed0 - R(0.2), R(0.2)));
+    if (h0v < K.h0x9 || totsed0 < R(0.2)) dfmask = 0;
+    R betax = K.neg1ml * gz * h0v * K.fa;
+    R betay = K.neg1ml * gz * h0v * K.fa;
     if (hu0 < 0) betax = -1 * betax;
     if (hv0 < 0) betay = -1 * betay;
 
     /* Hairsine-Rose, class-independent parts (SWEHR.c:1330-1382) */
-    const double hvert = h0v / sw_cos_atan(fabs(slope));
-    double mtstar = P.mtstar0;
-    const bool deepv = hvert > P.h0;
-    double depthfac = 1.0;
+    const R hvert = PP::div(h0v, PP::cos_atan(fabs(slope)));
+    R mtstar = K.mtstar0;
+    const bool deepv = hvert > K.h0;
+    R depthfac = 1;
     if (deepv) {
-        depthfac = sw_pow(P.h0 / hvert, P.b);
-        mtstar = P.mtstar0 * depthfac;
+        depthfac = PP::pow(PP::div(K.h0, hvert), K.b);
+        mtstar = K.mtstar0 * depthfac;
     }
-    const double Hs = fmin(1.0, totm0 / mtstar);
-    const bool swash = (h0v > P.hfx10 && totsed0 < 0.6);
-    double E3b = 0, E4b = 0, e4den = 1;
+    const R Hs = fmin(one, PP::div(totm0, mtstar));
+    const bool swash = (h0v > K.hfx10 && totsed0 < R(0.6));
+    R E3b = 0, E4b = 0, e4den = 1;
     if (swash) {
-        const double manning = (h0v <= P.hc) ? P.roughness * sw_pow(h0v / P.hc, P.dde) : P.roughness;
-        const double qq = sw_sqrt_pow(hu0 * hu0 + hv0 * hv0);
-        const double SF = manning * manning * qq * qq / sw_pow(h0v, 3.333);
+        const R manning = (h0v <= K.hc) ? K.roughness * PP::pow(PP::div(h0v, K.hc), K.dde) : K.roughness;
+        const R qq = PP::sqrtp(hu0 * hu0 + hv0 * hv0);
+        const R SF = PP::div(manning * manning * qq * qq, PP::pow(h0v, R(3.333)));
         /* streampowererosion (SWEHR.c:412-426): omega is the same for every
          * class; only the h > d_k condition differs */
-        const double omega = rho0c * gz * SF * qq;
-        if (omega > P.uc && totsed0 < 0.6) E3b = P.af * (omega - P.uc);
-        if (omega > P.uc2 && totsed0 < 0.6) E4b = P.afr * (omega - P.uc2);
-        e4den = (rhos - rho0c) / rhos * gz * h0v;
+        const R omega = rho0c * gz * SF * qq;
+        if (omega > K.uc && totsed0 < R(0.6)) E3b = K.af * (omega - K.uc);
+        if (omega > K.uc2 && totsed0 < R(0.6)) E4b = K.afr * (omega - K.uc2);
+        e4den = PP::div(rhos - rho0c, rhos) * gz * h0v;
     }
-    const double vfconc = sw_pow(1 - fmin(totsed0, 0.99), 4.0);
-    const bool debris = (h0v > P.h0x9 && totsed0 > P.cthreshold);
+    const R vfconc = PP::pow(1 - fmin(totsed0, R(0.99)), R(4.0));
+    const bool debris = (h0v > K.h0x9 && totsed0 > K.cthreshold);
 
-    /* conservative update + Green-Ampt, SWEHR.c:1424-1452 */
-    const double dtdx = dt * P.oneoverdx;
-    double h = h0v - dtdx * (fxr0 - fxl0) - dtdx * (fyr0 - fyl0) + dt * Rc;
-    double hu = hu0 - dtdx * (fxr1 - fxl1) - dtdx * (fyr1 - fyl1) + dt * SXf + dt * gammax + dt * dfmask * betax;
-    double hv = hv0 - dtdx * (fxr2 - fxl2) - dtdx * (fyr2 - fyl2) + dt * SYf + dt * gammay + dt * dfmask * betay;
-    const double ks = P.has_ks ? ksf[q] : P.ks;
-    const double vinf0 = src[P_VINF * pl + q];
+    /* conservative update, SWEHR.c:1424-1446 */
+    const R dtdx = dtr * K.oneoverdx;
+    R h = h0v - dtdx * (fxr0 - fxl0) - dtdx * (fyr0 - fyl0) + dtr * Rc;
+    R hu = hu0 - dtdx * (fxr1 - fxl1) - dtdx * (fyr1 - fyl1) + dtr * SXf + dtr * gammax + dtr * dfmask * betax;
+    R hv = hv0 - dtdx * (fxr2 - fxl2) - dtdx * (fyr2 - fyl2) + dtr * SYf + dtr * gammay + dtr * dfmask * betay;
+    /* Green-Ampt in FP64 (SWEHR.c:1449-1452) */
+    const double ks = P.has_ks ? (double)cellr[CR_KS * T_I * T_J + cs] : P.ks;
+    const double vinf0 = celld[CD_VINF * T_I * T_J + cs];
     const double zf = vinf0 / (P.thetas - P.theta0);
-    const double infl = fmin(h - hfilm, dt * ks * (zf + P.hf + h) / zf);
+    const double hd = (double)h;
+    const double infl = fmin(hd - P.hfilm, dt * ks * (zf + P.hf + hd) / zf);
     const double vinf = vinf0 + infl;
-    h -= infl;
+    h = (R)(hd - infl);
 
     /* classes (SWEHR.c:1454-1511) */
-    const double *SED = sm + TL.sed;
-    double Uk[MAXS];
+    const R *SED = reinterpret_cast<const R *>(smb + L.sed);
+    R Uk[MAXS];
 #pragma unroll
     for (int k = 0; k < MAXS; k++) {
         if (k >= S) break;
-        const double *sk = SED + k * N_H;
-        Uk[k] = src[(P_FIXED + k) * pl + q] - dtdx * (fxr0 * sk[uxr] - fxl0 * sk[uxl])
+        const R *sk = SED + k * N_H;
+        Uk[k] = (R)halo[((HP_U + k) * HALO_ROWS) * R_J + so] - dtdx * (fxr0 * sk[uxr] - fxl0 * sk[uxl])
                 - dtdx * (fyr0 * sk[uyr] - fyl0 * sk[uyl]);
     }
-    double z = zc[q];
-    double totm = 0, dep = 0, chtemp = 0, bulk = 0;
+    double z = zcs[(ti + 1) * R_J + (tj + 2)];
+    double totm = 0, dep = 0;
+    R chtemp = 0, bulk = 0;
 #pragma unroll
     for (int k = 0; k < MAXS; k++) {
         if (k >= S) break;
-        const int64_t qm = (P_FIXED + S + k) * pl + q;
-        const double Mk0 = src[qm];
-        double E1 = 0, E2 = 0, E3 = 0, E4 = 0;
+        const int64_t qm = k * pl + q;
+        const double Mk0 = celld[(CD_M + k) * T_I * T_J + cs];
+        const R Mk0r = (R)Mk0;
+        R E1 = 0, E2 = 0, E3 = 0, E4 = 0;
         if (swash) {
-            E1 = (1 - Hs) * P.pf[k] * P.a * Rc;
-            if (totm0 > 1e-8 && Mk0 > 1e-8) E2 = Hs * Mk0 / totm0 * P.ad * Rc;
+            E1 = (1 - Hs) * K.pf[k] * K.a * Rc;
+            if (totm0 > R(1e-8) && Mk0r > R(1e-8)) E2 = PP::div(Hs * Mk0r, totm0) * K.ad * Rc;
             if (deepv) { E1 = E1 * depthfac; E2 = E2 * depthfac; }
-            E3 = (1 - Hs) * P.pf[k] * P.F / P.J * (h0v > P.ds[k] ? E3b : 0.0);
-            if (totm0 > 1e-6 && Mk0 > 0)
-                E4 = P.one_m_bb * Hs * Mk0 / totm0 * P.F / e4den * (h0v > P.ds[k] ? E4b : 0.0);
+            E3 = PP::div((1 - Hs) * K.pf[k] * K.F, K.J) * (h0v > K.ds[k] ? E3b : R(0));
+            if (totm0 > R(1e-6) && Mk0r > 0)
+                E4 = PP::div(PP::div(K.one_m_bb * Hs * Mk0r, totm0) * K.F, e4den) * (h0v > K.ds[k] ? E4b : R(0));
         }
-        double VF = sw_sqrt_pow(P.a13sq[k] + P.c109s * gz * P.ds[k]) - P.a13[k];
+        R VF = PP::settle(K.a13[k], K.a13sq[k], K.c109s * gz * K.ds[k]);
         VF = VF * vfconc;
-        if (P.ds[k] > 0.0001 && h0v < P.h0x9) VF = 2e-3 + fmax(h0v - P.h0x3, 0.0) * (VF - 2e-3) / P.h0x6;
-        if (P.ds[k] > 0.002 && h0v < P.h0x9) VF = 2e-3 + fmax(h0v - P.h0x3, 0.0) * (VF - 2e-3) / P.h0x6;
+        if (K.ds[k] > R(0.0001) && h0v < K.h0x9) VF = R(2e-3) + PP::div(fmax(h0v - K.h0x3, R(0)) * (VF - R(2e-3)), K.h0x6);
+        if (K.ds[k] > R(0.002) && h0v < K.h0x9) VF = R(2e-3) + PP::div(fmax(h0v - K.h0x3, R(0)) * (VF - R(2e-3)), K.h0x6);
         if (debris) { E1 = E2 = E3 = E4 = 0; VF = 0; }
 
         double Mk = Mk0;
-        double u = Uk[k];
-        if (h < P.hfx10) {
-            Mk += dt * E1 + u;
+        R u = Uk[k];
+        double det_k = 0;         /* original soil detached into U_k + M_k this step (budget) */
+        if (h < K.hfx10) {
+            Mk += (double)(dtr * E1 + u);
             u = 0;
-            if (BUDGET) acc.det[k] += dt * E1;
+            if (BUDGET) det_k = (double)(dtr * E1);
         } else {
             chtemp = u;
-            const double redetach = fmin(Mk, dt * (E2 + E4));
-            const double dec = sw_exp(-VF / h * (0.5 * dt));
+            const R redetach = fmin(Mk0r, dtr * (E2 + E4));
+            const R dec = PP::exp(PP::div(-VF, h) * (half * dtr));
             u = dec * u;
-            u = u + dt * (E1 + E3) + redetach;
+            u = u + dtr * (E1 + E3) + redetach;
             u = dec * u;
-            z = z - P.invporo * (u - chtemp);
-            Mk = Mk + dt * (E1 + E3) - (u - chtemp);
-            if (BUDGET) acc.det[k] += dt * (E1 + E3);
+            z = z - P.invporo * (double)(u - chtemp);
+            Mk = Mk + (double)(dtr * (E1 + E3)) - (double)(u - chtemp);
+            if (BUDGET) det_k = (double)(dtr * (E1 + E3));
             if (fail == 1) {
                 z = z - 0.99 * Mk / P.porod;
-                u = u + 0.99 * Mk;
+                u = u + (R)(0.99 * Mk);
                 totm = 0;
                 Mk = 0.01 * Mk;
                 dep = 0;
             }
         }
-        const double dh = (u - chtemp) / P.porod;
+        const R dh = PP::div(u - chtemp, K.porod);
         h = h + dh;
         bulk += dh;
         totm += Mk;
-        dep += Mk / rhos;
+        dep += Mk / P.rhos;
         Uk[k] = u;
-        dst[qm] = Mk;
+        dst.M[qm] = Mk;
+        if (BUDGET) {
+            /* U_k + M_k changes only by the face fluxes and detachment; what
+             * the arithmetic and storage add on top is accounted as rounding */
+            const R *sk = SED + k * N_H;
+            const double div = ((double)(fxr0 * sk[uxr]) - (double)(fxl0 * sk[uxl]))
+                               + ((double)(fyr0 * sk[uyr]) - (double)(fyl0 * sk[uyl]));
+            const double change = ((double)(RS)u - (double)halo[((HP_U + k) * HALO_ROWS) * R_J + so]) + (Mk - Mk0);
+            acc.det[k] += det_k;
+            acc.sround[k] += change - (-(dt * P.oneoverdx) * div + det_k);
+        }
     }
 
     /* derived fields and the dry clamp, SWEHR.c:1513-1551 */
-    double totsed = 0, clamp = 0;
+    R totsed = 0, clamp = 0;
     if (h > hfilm) {
 #pragma unroll
         for (int k = 0; k < MAXS; k++) {
             if (k >= S) break;
-            totsed += (Uk[k] / h) / rhos;
-            dst[(P_FIXED + k) * pl + q] = Uk[k];
+            totsed += PP::div(PP::div(Uk[k], h), rhos);
+            dst.U[k * pl + q] = (RS)Uk[k];
         }
     } else {
         clamp = hfilm - h;
@@ -525,63 +780,71 @@ __device__ __forceinline__ void tile_cell(const DevParams &P, const double *__re
 #pragma unroll
         for (int k = 0; k < MAXS; k++) {
             if (k >= S) break;
-            const int64_t qm = (P_FIXED + S + k) * pl + q;
-            z = z + P.invporo * Uk[k];
-            dst[qm] = dst[qm] + Uk[k];
-            dst[(P_FIXED + k) * pl + q] = 0.0;
+            const int64_t qm = k * pl + q;
+            z = z + P.invporo * (double)Uk[k];
+            dst.M[qm] = dst.M[qm] + (double)Uk[k];
+            dst.U[qm] = (RS)0;
         }
     }
     /* implicit friction, SWEHR.c:1553-1565 */
-    double vel1 = 0, vel2 = 0;
+    R vel1 = 0, vel2 = 0;
     if (h > hfilm) {
-        const double manning = (h <= P.hc) ? P.roughness * sw_pow(h / P.hc, P.dde) : P.roughness;
-        const double SFf = manning * manning * gz * sw_sqrt_pow(hu * hu + hv * hv) * 1 / sw_pow(h, 2.333);
-        hu = hu / (1 + dt * SFf);
-        hv = hv / (1 + dt * SFf);
-        vel1 = hu / h;
-        vel2 = hv / h;
+        const R manning = (h <= K.hc) ? K.roughness * PP::pow(PP::div(h, K.hc), K.dde) : K.roughness;
+        const R SFf = PP::div(manning * manning * gz * PP::sqrtp(hu * hu + hv * hv) * 1, PP::pow(h, R(2.333)));
+        hu = PP::div(hu, 1 + dtr * SFf);
+        hv = PP::div(hv, 1 + dtr * SFf);
+        vel1 = PP::div(hu, h);
+        vel2 = PP::div(hv, h);
     }
-    double maxvel = src[P_MAXVEL * pl + q], maxdep = src[P_MAXDEP * pl + q];
-    const double vmag = sw_sqrt_pow(vel1 * vel1 + vel2 * vel2);
+    R maxvel = (R)cellr[CR_MAXVEL * T_I * T_J + cs], maxdep = (R)cellr[CR_MAXDEP * T_I * T_J + cs];
+    const R vmag = PP::sqrtp(vel1 * vel1 + vel2 * vel2);
     if (vmag > maxvel) maxvel = vmag;
     if (h > maxdep) maxdep = h;
-    dst[P_H * pl + q] = h;
-    dst[P_HU * pl + q] = hu;
-    dst[P_HV * pl + q] = hv;
-    dst[P_VINF * pl + q] = vinf;
-    dst[P_MAXVEL * pl + q] = maxvel;
-    dst[P_MAXDEP * pl + q] = maxdep;
-    dst[P_TOTM * pl + q] = totm;
-    dst[P_DEP * pl + q] = dep;
-    dst[P_TOTSED * pl + q] = totsed;
+    dst.h[q] = (RS)h;
+    dst.hu[q] = (RS)hu;
+    dst.hv[q] = (RS)hv;
+    dst.vinf[q] = vinf;
+    dst.maxvel[q] = (RS)maxvel;
+    dst.maxdep[q] = (RS)maxdep;
+    dst.totm[q] = (RS)totm;
+    dst.dep[q] = (RS)dep;
+    dst.totsed[q] = (RS)totsed;
     zn[q] = z;
 
     if (BUDGET) {
-        acc.rain += dt * Rc;
+        /* water: the state changes by the face fluxes, rain, infiltration,
+         * bulking and the dry clamp; the arithmetic and storage rounding of h
+         * is accounted separately so the budget closes exactly */
+        const double dtdx_d = dt * P.oneoverdx;
+        const double div = ((double)fxr0 - (double)fxl0) + ((double)fyr0 - (double)fyl0);
+        const double accounted = -dtdx_d * div + dt * (double)Rc - infl + (double)bulk + (double)clamp;
+        acc.round += ((double)(RS)h - (double)h0v) - accounted;
+        acc.rain += dt * (double)Rc;
         acc.inf += infl;
-        acc.clamp += clamp;
-        acc.bulk += bulk;
+        acc.clamp += (double)clamp;
+        acc.bulk += (double)bulk;
         if (i == 1 || i == P.nx || j == 1 || j == P.ny) {
 #pragma unroll
             for (int k = 0; k < MAXS; k++) {
                 if (k >= S) break;
-                const double *sk = SED + k * N_H;
-                if (i == 1) acc.sout[k] -= dtdx * (fxl0 * sk[uxl]);
-                if (i == P.nx) acc.sout[k] += dtdx * (fxr0 * sk[uxr]);
-                if (j == 1) acc.sout[k] -= dtdx * (fyl0 * sk[uyl]);
-                if (j == P.ny) acc.sout[k] += dtdx * (fyr0 * sk[uyr]);
+                const R *sk = SED + k * N_H;
+                if (i == 1) acc.sout[k] -= dtdx_d * (double)(fxl0 * sk[uxl]);
+                if (i == P.nx) acc.sout[k] += dtdx_d * (double)(fxr0 * sk[uxr]);
+                if (j == 1) acc.sout[k] -= dtdx_d * (double)(fyl0 * sk[uyl]);
+                if (j == P.ny) acc.sout[k] += dtdx_d * (double)(fyr0 * sk[uyr]);
             }
-            if (i == 1) acc.out -= dtdx * fxl0;
-            if (i == P.nx) acc.out += dtdx * fxr0;
-            if (j == 1) acc.out -= dtdx * fyl0;
-            if (j == P.ny) acc.out += dtdx * fyr0;
+            if (i == 1) acc.out -= dtdx_d * (double)fxl0;
+            if (i == P.nx) acc.out += dtdx_d * (double)fxr0;
+            if (j == 1) acc.out -= dtdx_d * (double)fyl0;
+            if (j == P.ny) acc.out += dtdx_d * (double)fyr0;
         }
     }
 }
 
 /* stage row of SWEHR.c:1593-1676 from the new state (one block) */
-__device__ __forceinline__ void stage_sample_tile(const DevParams &P, const double *__restrict__ st, Ctl *ctl, double tnew,
-                                  double *stage, double *saveflow, double *scratch)
+template <class PP, class RS>
+__device__ __forceinline__ void stage_sample_tile(const DevParams &P, const SetV<RS> &st, Ctl *ctl, double tnew,
+                                                  double *stage, double *saveflow, double *scratch)
 {
     double *bv = scratch;
     int *bi = reinterpret_cast<int *>(scratch + TILE_THREADS);
@@ -590,7 +853,7 @@ __device__ __forceinline__ void stage_sample_tile(const DevParams &P, const doub
     double best = 0;
     int besti = 1;
     for (int i = 1 + threadIdx.x; i <= P.nx; i += blockDim.x) {
-        const double h = st[P_H * pl + cidx(P, i, row)];
+        const double h = (double)st.h[cidx(P, i, row)];
         if (h > best) { best = h; besti = i; }
     }
     bv[threadIdx.x] = best;
@@ -604,15 +867,15 @@ __device__ __forceinline__ void stage_sample_tile(const DevParams &P, const doub
     const int64_t r = ctl->stagecnt;
     double *row_out = stage + r * 24;
     const int64_t qo = cidx(P, outlet, row);
-    const double ho = st[P_H * pl + qo];
-    const double v1 = ho > P.hfilm ? st[P_HU * pl + qo] / ho : 0, v2 = ho > P.hfilm ? st[P_HV * pl + qo] / ho : 0;
+    const double ho = (double)st.h[qo];
+    const double v1 = ho > P.hfilm ? (double)st.hu[qo] / ho : 0, v2 = ho > P.hfilm ? (double)st.hv[qo] / ho : 0;
     row_out[0] = tnew;
     row_out[1] = ho;
     row_out[2] = sw_sqrt_pow(v1 * v1 + v2 * v2);
-    row_out[3] = st[P_TOTSED * pl + qo];
+    row_out[3] = (double)st.totsed[qo];
     for (int k = 0; k < 10; k++) {
-        row_out[4 + k] = (k < P.S) ? st[(P_FIXED + P.S + k) * pl + qo] : 0;
-        row_out[14 + k] = (k < P.S) ? st[(P_FIXED + k) * pl + qo] : 0;
+        row_out[4 + k] = (k < P.S) ? st.M[k * pl + qo] : 0;
+        row_out[14 + k] = (k < P.S) ? (double)st.U[k * pl + qo] : 0;
     }
     double *pr = saveflow + r * 18;
     for (int m = 0; m < 6; m++) {
@@ -622,82 +885,93 @@ __device__ __forceinline__ void stage_sample_tile(const DevParams &P, const doub
             continue;
         }
         const int64_t qp = cidx(P, xi, yj);
-        const double hp = st[P_H * pl + qp];
-        const double w1 = hp > P.hfilm ? st[P_HU * pl + qp] / hp : 0, w2 = hp > P.hfilm ? st[P_HV * pl + qp] / hp : 0;
+        const double hp = (double)st.h[qp];
+        const double w1 = hp > P.hfilm ? (double)st.hu[qp] / hp : 0, w2 = hp > P.hfilm ? (double)st.hv[qp] / hp : 0;
         pr[3 * m] = hp;
         pr[3 * m + 1] = sw_sqrt_pow(w1 * w1 + w2 * w2);
-        pr[3 * m + 2] = st[P_TOTSED * pl + qp];
+        pr[3 * m + 2] = (double)st.totsed[qp];
     }
     ctl->stagecnt = r + 1;
     ctl->stageinterval += P.stageint;
 }
 
-template <int MAXS, bool BUDGET>
-__global__ void __launch_bounds__(TILE_THREADS, 2) k_update_tile(const DevParams P, const Bufs B, Ctl *ctl,
+template <class PP, class RS, int MAXS, bool BUDGET>
+__global__ void __launch_bounds__(TILE_THREADS, PP::kMinBlocks) k_update_tile(const DevParams P, const BufsT<RS> B, Ctl *ctl,
                                                                   const double *__restrict__ rain, double *partials,
                                                                   double *stage, double *saveflow)
 {
+    typedef typename PP::R R;
     if (!ctl->pending) return;
-    extern __shared__ double sm[];
-    const TileLayout TL = TileLayout::make(P.S);
+    extern __shared__ __align__(16) unsigned char smb[];
+    const StagedLayout L = StagedLayout::make(P.S, sizeof(R), 1);
+    const RealC<R> &K = kc<R>(P);
     const int64_t n = ctl->step;
     const double t = ctl->t, dt = ctl->dt;
-    const double *src = B.set[n & 1];
-    double *dst = B.set[(n + 1) & 1];
+    const SetV<RS> src = B.set[n & 1];
+    const SetV<RS> dst = B.set[(n + 1) & 1];
     const double *zp = B.z[(n + 2) % 3], *zc = B.z[n % 3];
     double *zn = B.z[(n + 1) % 3];
     double inh = 0, inhv = 0, insed = 0;
     if (P.inflow) inflow_ghost(t, inh, inhv, insed);
     const double Rr = P.storm ? 0.0 : rain_at(P, rain, t);
     Acc2<MAXS, BUDGET> acc;
-    acc.rain = acc.out = acc.clamp = acc.bulk = acc.inf = 0;
+    acc.rain = acc.out = acc.clamp = acc.bulk = acc.inf = acc.round = 0;
 #pragma unroll
-    for (int k = 0; k < (BUDGET ? MAXS : 1); k++) acc.det[k] = acc.sout[k] = 0;
+    for (int k = 0; k < (BUDGET ? MAXS : 1); k++) acc.det[k] = acc.sout[k] = acc.sround[k] = 0;
     const int64_t ntiles = (int64_t)((P.nx + T_I - 1) / T_I) * ((P.ny + T_J - 1) / T_J);
-    unsigned char *upb = reinterpret_cast<unsigned char *>(sm + TL.up);
+    unsigned char *upb = smb + L.up;
+    const R *su = reinterpret_cast<const R *>(smb + L.u), *sv = reinterpret_cast<const R *>(smb + L.v);
+    const R *sg = reinterpret_cast<const R *>(smb + L.g), *sc = reinterpret_cast<const R *>(smb + L.c);
+    R *sfx = reinterpret_cast<R *>(smb + L.fx), *sfy = reinterpret_cast<R *>(smb + L.fy);
     for (int64_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
         const TileCoord tc = tile_coord(P, tile);
-        stage_halo<1>(P, src, zp, tc, sm, TL, inh, inhv, insed);
+        stage_load<RS, 1>(P, src, zp, zc, B.ks, tc, smb, L);
+        __pipeline_wait_prior(0);
         __syncthreads();
-        /* stage B: faces */
+        stage_derive<PP, RS, 1>(P, tc, smb, L, (R)inh, (R)inhv, (R)insed);
+        __syncthreads();
+        const RS *sh = staged_h<RS>(smb, L);
+        /* stage B: every face of the tile (SWEHR.c:1099-1230) */
         for (int f = threadIdx.x; f < N_FX + N_FY; f += TILE_THREADS) {
-            double T0, T1, T2;
+            R T0, T1, T2;
             if (f < N_FX) {
-                const int fi = f / T_J, fj = f % T_J;
+                const int fi = f / T_J, fj = f - fi * T_J;
                 const int gi = tc.i0 - 1 + fi, gj = tc.j0 + fj;
                 if (gj > P.ny || gi > P.nx) continue;
-                const int L = fi * H_J + fj + 1, R = L + H_J;
-                hllc_v(sm[TL.h + L], sm[TL.h + R], sm[TL.u + L], sm[TL.u + R], sm[TL.v + L], sm[TL.v + R],
-                       sm[TL.g + L], sm[TL.c + L], P.hfilm, T0, T1, T2);
-                double *F = sm + TL.fx + 3 * f;
+                const int Lh = fi * H_J + fj + 1, Rh = Lh + H_J;
+                hllc_v<PP>((R)sh[fi * R_J + fj + 2], (R)sh[(fi + 1) * R_J + fj + 2], su[Lh], su[Rh], sv[Lh], sv[Rh],
+                           sg[Lh], sc[Lh], K.hfilm, T0, T1, T2);
+                R *F = sfx + 3 * f;
                 F[0] = T0; F[1] = T1; F[2] = T2;
                 upb[f] = (T0 > 0) ? 0 : 1;
             } else {
                 const int f2 = f - N_FX;
-                const int fi = f2 / (T_J + 1), fj = f2 % (T_J + 1);
+                const int fi = f2 / (T_J + 1), fj = f2 - fi * (T_J + 1);
                 const int gi = tc.i0 + fi, gj = tc.j0 - 1 + fj;
                 if (gi > P.nx || gj > P.ny) continue;
-                const int L = (fi + 1) * H_J + fj, R = L + 1;
-                hllc_v(sm[TL.h + L], sm[TL.h + R], sm[TL.v + L], sm[TL.v + R], sm[TL.u + L], sm[TL.u + R],
-                       sm[TL.g + L], sm[TL.c + L], P.hfilm, T0, T1, T2);
-                double *F = sm + TL.fy + 3 * f2;
+                const int Lh = (fi + 1) * H_J + fj, Rh = Lh + 1;
+                hllc_v<PP>((R)sh[(fi + 1) * R_J + fj + 1], (R)sh[(fi + 1) * R_J + fj + 2], sv[Lh], sv[Rh], su[Lh],
+                           su[Rh], sg[Lh], sc[Lh], K.hfilm, T0, T1, T2);
+                R *F = sfy + 3 * f2;
                 F[0] = T0; F[1] = T2; F[2] = T1;
                 upb[f] = (T0 > 0) ? 0 : 1;
             }
         }
         __syncthreads();
-        tile_cell<MAXS, BUDGET>(P, src, dst, zp, zc, zn, B.ks, sm, TL, tc, t, dt, Rr, acc);
+        tile_cell<PP, RS, MAXS, BUDGET>(P, src, dst, zp, zc, zn, smb, L, tc, t, dt, Rr, acc);
         __syncthreads();
     }
     __shared__ bool last;
-    double *red = sm + TL.red;
+    double *red = reinterpret_cast<double *>(smb + L.red);
     if (BUDGET) {
         double v[B_NTERMS];
         v[B_RAIN] = acc.rain; v[B_OUT] = acc.out; v[B_CLAMP] = acc.clamp; v[B_BULK] = acc.bulk; v[B_INF] = acc.inf;
+        v[B_ROUND] = acc.round;
 #pragma unroll
         for (int k = 0; k < 16; k++) {
             v[B_DET + k] = (k < MAXS) ? acc.det[k < MAXS ? k : 0] : 0.0;
             v[B_SOUT + k] = (k < MAXS) ? acc.sout[k < MAXS ? k : 0] : 0.0;
+            v[B_SROUND + k] = (k < MAXS) ? acc.sround[k < MAXS ? k : 0] : 0.0;
         }
 #pragma unroll
         for (int m = 0; m < B_NTERMS; m++) {
@@ -735,7 +1009,7 @@ __global__ void __launch_bounds__(TILE_THREADS, 2) k_update_tile(const DevParams
     const double tnew = (ctl->cfl ? 2 * P.tend : t) + dt;
     const bool stage_due = tnew > ctl->stageinterval && ctl->stagecnt < ctl->stagecap;
     __syncthreads();
-    if (stage_due) stage_sample_tile(P, dst, ctl, tnew, stage, saveflow, sm);
+    if (stage_due) stage_sample_tile<PP, RS>(P, dst, ctl, tnew, stage, saveflow, reinterpret_cast<double *>(smb));
     __syncthreads();
     if (threadIdx.x == 0) {
         ctl->t = tnew;

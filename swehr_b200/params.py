@@ -75,6 +75,7 @@ class SwehrBudget(C.Structure):
         ("detach", C.c_double * MAX_CLASSES), ("sed_outflow", C.c_double * MAX_CLASSES),
         ("sed_residual", C.c_double * MAX_CLASSES),
         ("sclass", C.c_int32), ("valid", C.c_int32),
+        ("rounding", C.c_double), ("sed_rounding", C.c_double * MAX_CLASSES),
     ]
 
 
