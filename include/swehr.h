@@ -215,6 +215,69 @@ void swehr_destroy(swehr_ctx *ctx);
 int swehr_cfl_noalloc(const swehr_params *p, const double *d_h, const double *d_hu, const double *d_hv,
                       const double *d_zprev, int64_t pitch, double t, double *d_result, void *stream);
 
+/* ---- scenario pool: many independent simulations stepped together ------
+ * No reference counterpart (SWEHR.c runs one catchment per process).  Every
+ * resident scenario advances one of its own time steps per pool step; one
+ * pool step is two persistent launches over the tiles of all unfinished
+ * scenarios (CUDA graphs of 32 steps), so scenarios of any mix of sizes share
+ * the GPU.  Each scenario keeps its own dt, time, stage rows and budgets and
+ * computes exactly what it computes alone.  A scenario is admitted only when
+ * its device footprint fits the pool's HBM limit and a slot is free, stays
+ * resident until its event ends (t >= tend), its step limit or an error, and
+ * is read through the single-domain calls on the handle swehr_pool_scenario
+ * returns.  All pool calls are synchronous and not thread-safe. */
+typedef struct swehr_pool swehr_pool;
+
+typedef struct {
+    int32_t resident;        /* scenarios holding device memory */
+    int32_t running;         /* resident and not yet finished */
+    int32_t finished_now;    /* scenarios that finished during this call */
+    int32_t tuned;           /* 1 once the launch shape has been chosen */
+    int64_t pool_steps;      /* pool steps launched by this call */
+    int64_t cell_steps;      /* cells x steps advanced by this call */
+    double device_ms;        /* GPU time of this call */
+    size_t hbm_used, hbm_limit;
+    int32_t grid_wave, grid_update;   /* launch shape in use (blocks) */
+} swehr_pool_stats;
+
+/* precision: SWEHR_FP64 or SWEHR_MIXED for every scenario; max_classes:
+ * largest sclass admitted; budget: accumulate mass budgets for scenarios
+ * that ask for them; hbm_limit: admission limit in bytes for scenario state
+ * (0 = 90% of the device memory free now); max_scenarios: resident slots. */
+int swehr_pool_create(int precision, int max_classes, int budget, size_t hbm_limit, int max_scenarios,
+                      swehr_pool **out);
+
+/* Upload a scenario (t = 0, initial state as swehr_create) and add it to the
+ * batch; max_steps < 0 for no step limit.  SWEHR_BUSY when its footprint or
+ * a slot is not free now (nothing allocated: retry after a release);
+ * SWEHR_INVALID when it can never fit. */
+int swehr_pool_submit(swehr_pool *pool, const swehr_params *p, const swehr_inputs *in, int64_t max_steps,
+                      int *id);
+
+/* Advance every running scenario by up to `steps` pool steps (< 0: until all
+ * finish); returns after one synchronisation. */
+int swehr_pool_run(swehr_pool *pool, int64_t steps, swehr_pool_stats *stats);
+
+/* Launch-shape autotuner: times `steps_per_trial` real pool steps for each
+ * candidate persistent grid (1..occupancy blocks per SM for each kernel) and
+ * keeps the fastest per tile-step; the scenarios advance meanwhile. */
+int swehr_pool_tune(swehr_pool *pool, int64_t steps_per_trial, swehr_pool_stats *stats);
+
+/* progress of one scenario (status, done, t, steps) */
+int swehr_pool_poll(swehr_pool *pool, int id, swehr_progress *pr);
+
+/* The scenario's context for swehr_read_field / swehr_read_series /
+ * swehr_get_budget / swehr_write_field (not for swehr_advance or
+ * swehr_destroy). */
+int swehr_pool_scenario(swehr_pool *pool, int id, swehr_ctx **ctx);
+
+/* Free a scenario's device memory and slot (running or finished). */
+int swehr_pool_release(swehr_pool *pool, int id);
+
+int swehr_pool_stats_get(swehr_pool *pool, swehr_pool_stats *stats);
+
+void swehr_pool_destroy(swehr_pool *pool);
+
 #ifdef __cplusplus
 }
 #endif

@@ -27,6 +27,7 @@ SOURCES = [
     ("swehr_step_f64.cu", ["--fmad=false"]),
     ("swehr_step_f32.cu", []),
     ("swehr_capi.cu", []),
+    ("swehr_pool.cu", []),
     ("swehr_cfl_noalloc.cu", ["--fmad=false"]),
 ]
 
@@ -45,7 +46,7 @@ def build(verbose: bool = False, ptxas_v: bool = False) -> str:
         deps = [srcp] + [os.path.join(CSRC, f) for f in os.listdir(CSRC) if f.endswith((".h", ".cuh"))]
         deps.append(os.path.join(HERE, "..", "include", "swehr.h"))
         if not os.path.exists(obj) or any(os.path.getmtime(d) > os.path.getmtime(obj) for d in deps) or ptxas_v:
-            cmd = [nvcc()] + ARCH + COMMON + extra + ["-dc" if False else "-c", srcp, "-o", obj]
+            cmd = [nvcc()] + ARCH + COMMON + extra + ["-c", srcp, "-o", obj]
             if ptxas_v:
                 cmd += ["-Xptxas", "-v"]
             if verbose:

@@ -19,17 +19,19 @@
 #include <vector>
 
 #include "../../include/swehr.h"
-#include "swehr_kernels.h"
+#include "swehr_ctx.h"
 
 using namespace swehr;
 
 static thread_local std::string g_last_error;
 
-static int set_err(int code, const std::string &msg)
+int swehr_err(int code, const std::string &msg)
 {
     g_last_error = msg;
     return code;
 }
+
+static int set_err(int code, const std::string &msg) { return swehr_err(code, msg); }
 
 #define CK(call)                                                                                      \
     do {                                                                                              \
@@ -37,33 +39,6 @@ static int set_err(int code, const std::string &msg)
         if (e_ != cudaSuccess)                                                                        \
             return set_err(SWEHR_CUDA_ERROR, std::string(#call) + ": " + cudaGetErrorString(e_));     \
     } while (0)
-
-static const int GRAPH_STEPS = 32;
-static const int TIMING_RING = 64;
-
-struct swehr_ctx {
-    swehr_params p;
-    int precision = SWEHR_FP64;
-    int device = 0, num_sms = 148;
-    DevParams P;
-    BufsT<double> B64;      /* plain form */
-    BufsT<float> B32;       /* mixed form */
-    size_t rsize = 8;       /* bytes of a bulk (RS) element */
-    char *pool = nullptr;
-    size_t pool_bytes = 0;
-    double *d_rain = nullptr, *d_partials = nullptr, *d_stage = nullptr, *d_saveflow = nullptr;
-    Ctl *d_ctl = nullptr;
-    Ctl *h_ctl = nullptr;   /* pinned mirror */
-    cudaStream_t stream = nullptr;
-    cudaGraphExec_t graph = nullptr;
-    cudaEvent_t ev_start = nullptr, ev_stop = nullptr;
-    cudaEvent_t ev_k[2 * TIMING_RING] = {};
-    StepConfig cfg;
-    int timing = 0;
-    int64_t stagecap = 0;
-    double water_init = 0;
-    double sed_init[SWEHR_MAX_CLASSES] = {};
-};
 
 extern "C" {
 
@@ -304,13 +279,23 @@ static void destroy_ctx(swehr_ctx *c)
     if (c->ev_stop) cudaEventDestroy(c->ev_stop);
     for (int e = 0; e < 2 * TIMING_RING; e++)
         if (c->ev_k[e]) cudaEventDestroy(c->ev_k[e]);
-    if (c->pool) cudaFree(c->pool);
+    if (c->mem) cudaFree(c->mem);
     if (c->h_ctl) cudaFreeHost(c->h_ctl);
     if (c->stream) cudaStreamDestroy(c->stream);
     delete c;
 }
 
 extern "C" int swehr_create(const swehr_params *p, const swehr_inputs *in, int precision, swehr_ctx **out)
+{
+    return swehr_ctx_create(p, in, precision, 0, out);
+}
+
+size_t swehr_ctx_footprint(const swehr_params *p, int has_ks, int precision, int num_sms)
+{
+    return layout_for(p->nx, p->ny, p->sclass, p->rnum, has_ks, stagecap_for(p), num_sms * 4, precision).total;
+}
+
+int swehr_ctx_create(const swehr_params *p, const swehr_inputs *in, int precision, int pooled, swehr_ctx **out)
 {
     if (!out) return set_err(SWEHR_INVALID, "NULL out");
     *out = nullptr;
@@ -322,6 +307,7 @@ extern "C" int swehr_create(const swehr_params *p, const swehr_inputs *in, int p
     swehr_ctx *c = new swehr_ctx();
     c->p = *p;
     c->precision = precision;
+    c->pooled = pooled;
     int rc;
 #define CKC(call)                                                                               \
     do {                                                                                        \
@@ -353,20 +339,21 @@ extern "C" int swehr_create(const swehr_params *p, const swehr_inputs *in, int p
     c->rsize = L.rsize;
     make_devparams(p, in, L, c->P);
     CKC(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
-    CKC(cudaMalloc((void **)&c->pool, L.total));
-    c->pool_bytes = L.total;
-    CKC(cudaMemsetAsync(c->pool, 0, L.total, c->stream));
-    if (precision == SWEHR_MIXED) set_views(c->B32, c->pool, L, p->sclass, in->ks != nullptr, 1);
-    else set_views(c->B64, c->pool, L, p->sclass, in->ks != nullptr, 0);
-    c->d_rain = (double *)(c->pool + L.off_rain);
-    c->d_ctl = (Ctl *)(c->pool + L.off_ctl);
-    c->d_partials = (double *)(c->pool + L.off_partials);
-    c->d_stage = (double *)(c->pool + L.off_stage);
-    c->d_saveflow = (double *)(c->pool + L.off_saveflow);
+    CKC(cudaMalloc((void **)&c->mem, L.total));
+    c->mem_bytes = L.total;
+    CKC(cudaMemsetAsync(c->mem, 0, L.total, c->stream));
+    if (precision == SWEHR_MIXED) set_views(c->B32, c->mem, L, p->sclass, in->ks != nullptr, 1);
+    else set_views(c->B64, c->mem, L, p->sclass, in->ks != nullptr, 0);
+    c->d_rain = (double *)(c->mem + L.off_rain);
+    c->d_ctl = (Ctl *)(c->mem + L.off_ctl);
+    c->d_partials = (double *)(c->mem + L.off_partials);
+    c->d_stage = (double *)(c->mem + L.off_stage);
+    c->d_saveflow = (double *)(c->mem + L.off_saveflow);
     CKC(cudaMallocHost((void **)&c->h_ctl, sizeof(Ctl)));
     CKC(cudaEventCreate(&c->ev_start));
     CKC(cudaEventCreate(&c->ev_stop));
-    for (int e = 0; e < 2 * TIMING_RING; e++) CKC(cudaEventCreate(&c->ev_k[e]));
+    if (!pooled)
+        for (int e = 0; e < 2 * TIMING_RING; e++) CKC(cudaEventCreate(&c->ev_k[e]));
     /* initial state (initialcondition, SWEHR.c:211-285): dry bed, VINF = vinf0, z = topo;
      * z of the previous step = z (setup slopes, SWEHR.c:721-803) */
     double *const *zpl = precision == SWEHR_MIXED ? c->B32.z : c->B64.z;
@@ -401,11 +388,18 @@ extern "C" int swehr_create(const swehr_params *p, const swehr_inputs *in, int p
 #undef CKC
 }
 
-extern "C" void swehr_destroy(swehr_ctx *c) { destroy_ctx(c); }
+extern "C" void swehr_destroy(swehr_ctx *c)
+{
+    if (c && c->pooled) return;   /* owned by its pool: swehr_pool_release */
+    destroy_ctx(c);
+}
+
+void swehr_ctx_destroy(swehr_ctx *c) { destroy_ctx(c); }
 
 extern "C" int swehr_set_timing(swehr_ctx *c, int on)
 {
     if (!c) return set_err(SWEHR_INVALID, "NULL ctx");
+    if (c->pooled) return set_err(SWEHR_INVALID, "a pooled scenario is stepped by its pool");
     c->timing = on ? 1 : 0;
     return SWEHR_OK;
 }
@@ -435,6 +429,7 @@ static int build_graph(swehr_ctx *c)
 extern "C" int swehr_advance(swehr_ctx *c, double t_stop, int64_t max_steps, swehr_progress *pr)
 {
     if (!c) return set_err(SWEHR_INVALID, "NULL ctx");
+    if (c->pooled) return set_err(SWEHR_INVALID, "a pooled scenario is stepped by its pool");
     auto wall0 = std::chrono::steady_clock::now();
     /* read the control block, arm it */
     CK(cudaMemcpyAsync(c->h_ctl, c->d_ctl, sizeof(Ctl), cudaMemcpyDeviceToHost, c->stream));

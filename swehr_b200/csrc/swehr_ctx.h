@@ -1,0 +1,51 @@
+/*
+ * swehr_ctx.h -- host-side state of one simulation (internal to the library;
+ * shared by the single-domain entry points and the scenario pool).
+ */
+#pragma once
+#include <cuda_runtime.h>
+
+#include <string>
+
+#include "../../include/swehr.h"
+#include "swehr_kernels.h"
+
+static const int GRAPH_STEPS = 32;
+static const int TIMING_RING = 64;
+
+struct swehr_ctx {
+    swehr_params p;
+    int precision = SWEHR_FP64;
+    int device = 0, num_sms = 148;
+    int pooled = 0;         /* stepped by a swehr_pool, not by swehr_advance */
+    swehr::DevParams P;
+    swehr::BufsT<double> B64;      /* plain form */
+    swehr::BufsT<float> B32;       /* mixed form */
+    size_t rsize = 8;       /* bytes of a bulk (RS) element */
+    char *mem = nullptr;    /* the one device allocation */
+    size_t mem_bytes = 0;
+    double *d_rain = nullptr, *d_partials = nullptr, *d_stage = nullptr, *d_saveflow = nullptr;
+    swehr::Ctl *d_ctl = nullptr;
+    swehr::Ctl *h_ctl = nullptr;   /* pinned mirror */
+    cudaStream_t stream = nullptr;
+    cudaGraphExec_t graph = nullptr;
+    cudaEvent_t ev_start = nullptr, ev_stop = nullptr;
+    cudaEvent_t ev_k[2 * TIMING_RING] = {};
+    swehr::StepConfig cfg;
+    int timing = 0;
+    int64_t stagecap = 0;
+    double water_init = 0;
+    double sed_init[SWEHR_MAX_CLASSES] = {};
+};
+
+/* record an error message for swehr_last_error() and return code */
+int swehr_err(int code, const std::string &msg);
+
+/* Create a context; pooled contexts skip the single-domain timing events. */
+int swehr_ctx_create(const swehr_params *p, const swehr_inputs *in, int precision, int pooled, swehr_ctx **out);
+
+/* device bytes swehr_ctx_create() allocates for these inputs (upper bound) */
+size_t swehr_ctx_footprint(const swehr_params *p, int has_ks, int precision, int num_sms);
+
+/* free a context (pools use this for their scenarios) */
+void swehr_ctx_destroy(swehr_ctx *c);

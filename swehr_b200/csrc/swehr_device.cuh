@@ -63,6 +63,13 @@ template <>
 __device__ __forceinline__ const RealC<float> &kc<float>(const DevParams &P) { return P.kf; }
 
 /* Device control block of one simulation (one per scenario). */
+/* host-visible progress of one scenario of a batch, written when it ends a step */
+struct ScenSummary {
+    double t, dt, courant;
+    int64_t step;
+    int32_t status, active;
+};
+
 struct Ctl {
     double t;             /* time at the start of the pending step */
     double dt, courant;   /* time step of the pending step */
@@ -79,6 +86,7 @@ struct Ctl {
     int64_t stagecnt, stagecap;
     int64_t launches;
     double budget_hi[64], budget_lo[64];   /* running compensated budget sums */
+    double budget_step[64];                 /* this step's partials in batched mode */
     double sed0[16];
 };
 

@@ -23,6 +23,39 @@ struct BufsT {
     const RS *ks;
 };
 
+/* one scenario of a batch: everything its tiles need */
+template <class RS>
+struct ScenDesc {
+    DevParams P;
+    BufsT<RS> B;
+    Ctl *ctl;
+    const double *rain;
+    double *stage, *saveflow;
+    ScenSummary *sum;                /* this scenario's progress slot */
+    int64_t tile0, ntiles;           /* its range in the batch's tile list */
+};
+
+/* what a batched launch walks; lives in device memory so that a captured
+ * graph stays valid while scenarios join and leave */
+template <class RS>
+struct BatchHdr {
+    const ScenDesc<RS> *tab;
+    int32_t nscen, pad;
+    int64_t total_tiles;
+};
+
+/* the batched kernels of one form (both take one argument: the header) */
+struct BatchConfig {
+    void *fn_wave = nullptr, *fn_update = nullptr;
+    size_t smem_wave = 0, smem_update = 0;
+    int occ_wave = 1, occ_update = 1;   /* resident blocks per SM */
+    int threads = 0;                    /* threads per block */
+    int tile_i = 0, tile_j = 0;         /* cells per tile */
+};
+
+int configure_batch_f64(int max_classes, bool budget, BatchConfig &cfg);
+int configure_batch_f32(int max_classes, bool budget, BatchConfig &cfg);
+
 /* launch geometry of the step kernels of one simulation */
 struct StepConfig {
     int grid_wave = 1, grid_update = 1;

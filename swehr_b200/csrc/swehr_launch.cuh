@@ -54,6 +54,37 @@ struct FormLauncher {
         return 0;
     }
 
+    template <int MAXS, bool BUDGET>
+    static void *ubatch_fn() { return (void *)k_update_batch<PP, RS, MAXS, BUDGET>; }
+
+    static int configure_batch(int max_classes, bool budget, BatchConfig &cfg)
+    {
+        void *fu;
+        if (max_classes <= 4) fu = budget ? ubatch_fn<4, true>() : ubatch_fn<4, false>();
+        else if (max_classes <= 8) fu = budget ? ubatch_fn<8, true>() : ubatch_fn<8, false>();
+        else fu = budget ? ubatch_fn<16, true>() : ubatch_fn<16, false>();
+        void *fw = (void *)k_wave_batch<PP, RS>;
+        const size_t su = update_smem(max_classes), sw = wave_smem();
+        cudaError_t e = cudaFuncSetAttribute(fu, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)su);
+        if (e != cudaSuccess) return (int)e;
+        e = cudaFuncSetAttribute(fw, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sw);
+        if (e != cudaSuccess) return (int)e;
+        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&cfg.occ_update, fu, TILE_THREADS, su);
+        if (e != cudaSuccess) return (int)e;
+        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&cfg.occ_wave, fw, TILE_THREADS, sw);
+        if (e != cudaSuccess) return (int)e;
+        if (cfg.occ_update < 1) cfg.occ_update = 1;
+        if (cfg.occ_wave < 1) cfg.occ_wave = 1;
+        cfg.fn_update = fu;
+        cfg.fn_wave = fw;
+        cfg.smem_update = su;
+        cfg.smem_wave = sw;
+        cfg.threads = TILE_THREADS;
+        cfg.tile_i = T_I;
+        cfg.tile_j = T_J;
+        return 0;
+    }
+
     static int launch(const DevParams &P, const BufsT<RS> &B, Ctl *ctl, const double *rain, double *partials,
                       double *stage, double *saveflow, const StepConfig &cfg, cudaStream_t s, cudaEvent_t ev0,
                       cudaEvent_t ev1)

@@ -21,4 +21,9 @@ int launch_step_f32(const DevParams &P, const BufsT<float> &B, Ctl *ctl, const d
     return FormLauncher<PolicyF32, float>::launch(P, B, ctl, rain, partials, stage, saveflow, cfg, s, ev0, ev1);
 }
 
+int configure_batch_f32(int max_classes, bool budget, BatchConfig &cfg)
+{
+    return FormLauncher<PolicyF32, float>::configure_batch(max_classes, budget, cfg);
+}
+
 }  // namespace swehr

@@ -33,4 +33,9 @@ int launch_step_f64(const DevParams &P, const BufsT<double> &B, Ctl *ctl, const 
     return FormLauncher<PolicyF64, double>::launch(P, B, ctl, rain, partials, stage, saveflow, cfg, s, ev0, ev1);
 }
 
+int configure_batch_f64(int max_classes, bool budget, BatchConfig &cfg)
+{
+    return FormLauncher<PolicyF64, double>::configure_batch(max_classes, budget, cfg);
+}
+
 }  // namespace swehr

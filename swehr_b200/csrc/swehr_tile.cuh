@@ -251,7 +251,8 @@ __device__ __forceinline__ void cp_pair(void *dst, const T *src)
 }
 
 /* Issue the tile's asynchronous copies.  WHAT = 0: wave pass (h hu hv, z_prev);
- * 1: update pass (all). */
+ * 1: update pass (all).  Each thread owns fixed (row, pair) slots and walks
+ * the planes with a pointer step, so the per-copy cost is one add. */
 template <class RS, int WHAT>
 __device__ __forceinline__ void stage_load(const DevParams &P, const SetV<RS> &src, const double *__restrict__ zp,
                                            const double *__restrict__ zc, const RS *__restrict__ ks, TileCoord tc,
@@ -259,47 +260,58 @@ __device__ __forceinline__ void stage_load(const DevParams &P, const SetV<RS> &s
 {
     const int64_t pl = P.plane;
     const int c0 = tc.j0 - 3;                                  /* 0-based grid column of staged column 0 */
-    /* halo planes: 10 rows x 18 pairs per plane */
-    RS *halo = reinterpret_cast<RS *>(smb + L.halo);
-    for (int job = threadIdx.x; job < L.nhalo * HALO_ROWS * (R_J / 2); job += TILE_THREADS) {
-        const int p = job / (HALO_ROWS * (R_J / 2));
-        const int rem = job - p * (HALO_ROWS * (R_J / 2));
-        const int r = rem / (R_J / 2), k2 = rem - r * (R_J / 2);
+    const int tid = threadIdx.x;
+    /* halo planes: 10 rows x 18 pairs = 180 slots */
+    if (tid < HALO_ROWS * (R_J / 2)) {
+        const int r = tid / (R_J / 2), k2 = tid - r * (R_J / 2);
         const int gi = tc.i0 - 1 + r, col = c0 + 2 * k2;
-        if (gi < 1 || gi > P.nx || col < 0 || col >= P.pitch) continue;
-        cp_pair(halo + (p * HALO_ROWS + r) * R_J + 2 * k2, halo_plane_src(src, p, pl) + (int64_t)(gi - 1) * P.pitch + col);
+        if (gi >= 1 && gi <= P.nx && col >= 0 && col < P.pitch) {
+            const int64_t go = (int64_t)(gi - 1) * P.pitch + col;
+            RS *d = reinterpret_cast<RS *>(smb + L.halo) + r * R_J + 2 * k2;
+            const int ps = HALO_ROWS * R_J;
+            cp_pair(d + HP_H * ps, src.h + go);
+            cp_pair(d + HP_HU * ps, src.hu + go);
+            cp_pair(d + HP_HV * ps, src.hv + go);
+            if (WHAT) {
+                cp_pair(d + HP_TS * ps, src.totsed + go);
+                cp_pair(d + HP_DEP * ps, src.dep + go);
+                const RS *u = src.U + go;
+                for (int k = 0; k < P.S; k++) cp_pair(d + (HP_U + k) * ps, u + (int64_t)k * pl);
+            }
+        }
     }
-    /* topography: z_prev rows i0-2.., z rows i0-1.. */
-    double *zps = reinterpret_cast<double *>(smb + L.zp);
-    double *zcs = reinterpret_cast<double *>(smb + L.zc);
-    const int nz = (ZP_ROWS + (WHAT ? ZC_ROWS : 0)) * (R_J / 2);
-    for (int job = threadIdx.x; job < nz; job += TILE_THREADS) {
-        const bool isp = job < ZP_ROWS * (R_J / 2);
-        const int j2 = isp ? job : job - ZP_ROWS * (R_J / 2);
-        const int r = j2 / (R_J / 2), k2 = j2 - r * (R_J / 2);
-        const int gi = (isp ? tc.i0 - 2 : tc.i0 - 1) + r, col = c0 + 2 * k2;
-        if (gi < 1 || gi > P.nx || col < 0 || col >= P.pitch) continue;
-        cp_pair((isp ? zps : zcs) + r * R_J + 2 * k2, (isp ? zp : zc) + (int64_t)(gi - 1) * P.pitch + col);
+    /* topography: z_prev 12 rows, z 10 rows, 18 pairs each */
+    {
+        const int slot = tid < HALO_ROWS * (R_J / 2) ? tid + (256 - HALO_ROWS * (R_J / 2)) : tid - HALO_ROWS * (R_J / 2);
+        const int nzs = (ZP_ROWS + (WHAT ? ZC_ROWS : 0)) * (R_J / 2);      /* 396 or 216 */
+        for (int s = slot; s < nzs; s += TILE_THREADS) {
+            const bool isp = s < ZP_ROWS * (R_J / 2);
+            const int s2 = isp ? s : s - ZP_ROWS * (R_J / 2);
+            const int r = s2 / (R_J / 2), k2 = s2 - r * (R_J / 2);
+            const int gi = (isp ? tc.i0 - 2 : tc.i0 - 1) + r, col = c0 + 2 * k2;
+            if (gi < 1 || gi > P.nx || col < 0 || col >= P.pitch) continue;
+            double *d = reinterpret_cast<double *>(smb + (isp ? L.zp : L.zc)) + r * R_J + 2 * k2;
+            cp_pair(d, (isp ? zp : zc) + (int64_t)(gi - 1) * P.pitch + col);
+        }
     }
     if (WHAT) {
-        /* cell planes: 8 rows x 16 pairs */
-        RS *cr = reinterpret_cast<RS *>(smb + L.cell_r);
-        double *cd = reinterpret_cast<double *>(smb + L.cell_d);
-        const int nr = (P.has_ks ? 4 : 3), njob = (nr + L.ncelld) * T_I * (T_J / 2);
-        for (int job = threadIdx.x; job < njob; job += TILE_THREADS) {
-            const int p = job / (T_I * (T_J / 2));
-            const int rem = job - p * (T_I * (T_J / 2));
-            const int r = rem / (T_J / 2), k2 = rem - r * (T_J / 2);
+        /* cell planes: 8 rows x 16 pairs = 128 slots; threads 128..255 */
+        if (tid >= TILE_THREADS - T_I * (T_J / 2)) {
+            const int s = tid - (TILE_THREADS - T_I * (T_J / 2));
+            const int r = s / (T_J / 2), k2 = s - r * (T_J / 2);
             const int gi = tc.i0 + r, col = tc.j0 - 1 + 2 * k2;
-            if (gi > P.nx || col >= P.pitch) continue;
-            const int64_t go = (int64_t)(gi - 1) * P.pitch + col;
-            if (p < nr) {
-                const RS *sp = p == CR_TOTM ? src.totm : p == CR_MAXVEL ? src.maxvel : p == CR_MAXDEP ? src.maxdep : ks;
-                cp_pair(cr + (p * T_I + r) * T_J + 2 * k2, sp + go);
-            } else {
-                const int d = p - nr;
-                const double *sp = d == CD_VINF ? src.vinf : src.M + (int64_t)(d - CD_M) * pl;
-                cp_pair(cd + (d * T_I + r) * T_J + 2 * k2, sp + go);
+            if (gi <= P.nx && col < P.pitch) {
+                const int64_t go = (int64_t)(gi - 1) * P.pitch + col;
+                RS *cr = reinterpret_cast<RS *>(smb + L.cell_r) + r * T_J + 2 * k2;
+                double *cd = reinterpret_cast<double *>(smb + L.cell_d) + r * T_J + 2 * k2;
+                const int ps = T_I * T_J;
+                cp_pair(cr + CR_TOTM * ps, src.totm + go);
+                cp_pair(cr + CR_MAXVEL * ps, src.maxvel + go);
+                cp_pair(cr + CR_MAXDEP * ps, src.maxdep + go);
+                if (P.has_ks) cp_pair(cr + CR_KS * ps, ks + go);
+                cp_pair(cd + CD_VINF * ps, src.vinf + go);
+                const double *m = src.M + go;
+                for (int k = 0; k < P.S; k++) cp_pair(cd + (CD_M + k) * ps, m + (int64_t)k * pl);
             }
         }
     }
@@ -396,73 +408,69 @@ __device__ __forceinline__ const RS *staged_h(const unsigned char *smb, const St
 }
 
 /* ------------------------------------------------------------------ wave */
+/* Largest wave speed over the faces a tile owns: i+1/2 and j+1/2 of its
+ * cells plus the domain's low boundary faces 1/2 (SWEHR.c:1092-1230's Smax).
+ * The whole block calls it; every thread returns its own partial max. */
 template <class PP, class RS>
-__global__ void __launch_bounds__(TILE_THREADS) k_wave_tile(const DevParams P, const BufsT<RS> B, Ctl *ctl)
+__device__ __forceinline__ typename PP::R wave_tile(const DevParams &P, const SetV<RS> &src,
+                                                    const double *__restrict__ zp, TileCoord tc, unsigned char *smb,
+                                                    const StagedLayout &L, double t)
 {
     typedef typename PP::R R;
-    if (!ctl->active) return;
-    extern __shared__ __align__(16) unsigned char smb[];
-    const StagedLayout L = StagedLayout::make(0, sizeof(R), 0);
     const RealC<R> &K = kc<R>(P);
-    const int64_t n = ctl->step;
-    const double t = ctl->t;
-    const SetV<RS> src = B.set[n & 1];
-    const double *zp = B.z[(n + 2) % 3];
     double inh = 0, inhv = 0, insed = 0;
     if (P.inflow) inflow_ghost(t, inh, inhv, insed);
-    const int64_t ntiles = (int64_t)((P.nx + T_I - 1) / T_I) * ((P.ny + T_J - 1) / T_J);
     const R *su = reinterpret_cast<const R *>(smb + L.u), *sv = reinterpret_cast<const R *>(smb + L.v);
     const R *sg = reinterpret_cast<const R *>(smb + L.g), *sc = reinterpret_cast<const R *>(smb + L.c);
+    stage_load<RS, 0>(P, src, zp, nullptr, nullptr, tc, smb, L);
+    __pipeline_wait_prior(0);
+    __syncthreads();
+    stage_derive<PP, RS, 0>(P, tc, smb, L, (R)inh, (R)inhv, (R)insed);
+    __syncthreads();
+    const RS *sh = staged_h<RS>(smb, L);
     R smax = 0;
-    for (int64_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
-        const TileCoord tc = tile_coord(P, tile);
-        stage_load<RS, 0>(P, src, zp, nullptr, nullptr, tc, smb, L);
-        __pipeline_wait_prior(0);
-        __syncthreads();
-        stage_derive<PP, RS, 0>(P, tc, smb, L, (R)inh, (R)inhv, (R)insed);
-        __syncthreads();
-        const RS *sh = staged_h<RS>(smb, L);
-        /* faces owned by the tile: i+1/2 and j+1/2 of its cells, plus the
-         * domain's low boundary faces 1/2 */
-        for (int f = threadIdx.x; f < N_FX + N_FY; f += TILE_THREADS) {
-            if (f < N_FX) {
-                const int fi = f / T_J, fj = f - fi * T_J;
-                const int gi = tc.i0 - 1 + fi, gj = tc.j0 + fj;
-                if (gj > P.ny || gi > P.nx || (fi == 0 && gi != 0)) continue;
-                const int Lh = fi * H_J + fj + 1, Rh = Lh + H_J;
-                const R s = hll_speed<PP>((R)sh[fi * R_J + fj + 2], (R)sh[(fi + 1) * R_J + fj + 2], su[Lh], su[Rh],
-                                          sg[Lh], sc[Lh], K.hfilm);
-                smax = (s > smax) ? s : smax;
-            } else {
-                const int f2 = f - N_FX;
-                const int fi = f2 / (T_J + 1), fj = f2 - fi * (T_J + 1);
-                const int gi = tc.i0 + fi, gj = tc.j0 - 1 + fj;
-                if (gi > P.nx || gj > P.ny || (fj == 0 && gj != 0)) continue;
-                const int Lh = (fi + 1) * H_J + fj, Rh = Lh + 1;
-                const R s = hll_speed<PP>((R)sh[(fi + 1) * R_J + fj + 1], (R)sh[(fi + 1) * R_J + fj + 2], sv[Lh],
-                                          sv[Rh], sg[Lh], sc[Lh], K.hfilm);
-                smax = (s > smax) ? s : smax;
-            }
+    for (int f = threadIdx.x; f < N_FX + N_FY; f += TILE_THREADS) {
+        if (f < N_FX) {
+            const int fi = f / T_J, fj = f - fi * T_J;
+            const int gi = tc.i0 - 1 + fi, gj = tc.j0 + fj;
+            if (gj > P.ny || gi > P.nx || (fi == 0 && gi != 0)) continue;
+            const int Lh = fi * H_J + fj + 1, Rh = Lh + H_J;
+            const R s = hll_speed<PP>((R)sh[fi * R_J + fj + 2], (R)sh[(fi + 1) * R_J + fj + 2], su[Lh], su[Rh],
+                                      sg[Lh], sc[Lh], K.hfilm);
+            smax = (s > smax) ? s : smax;
+        } else {
+            const int f2 = f - N_FX;
+            const int fi = f2 / (T_J + 1), fj = f2 - fi * (T_J + 1);
+            const int gi = tc.i0 + fi, gj = tc.j0 - 1 + fj;
+            if (gi > P.nx || gj > P.ny || (fj == 0 && gj != 0)) continue;
+            const int Lh = (fi + 1) * H_J + fj, Rh = Lh + 1;
+            const R s = hll_speed<PP>((R)sh[(fi + 1) * R_J + fj + 1], (R)sh[(fi + 1) * R_J + fj + 2], sv[Lh],
+                                      sv[Rh], sg[Lh], sc[Lh], K.hfilm);
+            smax = (s > smax) ? s : smax;
         }
-        __syncthreads();
-    }
-    __shared__ double red[TILE_THREADS / 32];
-    __shared__ bool last;
-    double smd = warp_max((double)smax);
-    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = smd;
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        double m = 0;
-        for (int w = 0; w < TILE_THREADS / 32; w++) m = (red[w] > m) ? red[w] : m;
-        atomicMax(&ctl->smax_bits, (unsigned long long)__double_as_longlong(m));
-        __threadfence();
-        unsigned tk = atomicAdd(&ctl->wave_ticket, 1u);
-        last = (tk == gridDim.x - 1);
     }
     __syncthreads();
-    if (!last || threadIdx.x != 0) return;
+    return smax;
+}
+
+/* block maximum of the threads' partial maxima (result valid in thread 0) */
+__device__ __forceinline__ double block_max(double v, double *red8)
+{
+    v = warp_max(v);
+    if ((threadIdx.x & 31) == 0) red8[threadIdx.x >> 5] = v;
+    __syncthreads();
+    double m = 0;
+    if (threadIdx.x == 0)
+        for (int w = 0; w < TILE_THREADS / 32; w++) m = (red8[w] > m) ? red8[w] : m;
+    __syncthreads();
+    return m;
+}
+
+/* CFL time step once every face of the step is in (SWEHR.c:1409-1413); one thread */
+__device__ __forceinline__ void wave_finalize(const DevParams &P, Ctl *ctl)
+{
     __threadfence();
-    /* CFL time step, SWEHR.c:1409-1413 */
+    const double t = ctl->t;
     const double Smax = __longlong_as_double((long long)atomicAdd(&ctl->smax_bits, 0ull));
     double dt = P.cstable * P.dx / Smax;
     if (dt > P.maxstep) dt = P.maxstep;
@@ -475,6 +483,36 @@ __global__ void __launch_bounds__(TILE_THREADS) k_wave_tile(const DevParams P, c
     ctl->wave_ticket = 0u;
     ctl->pending = 1;
 }
+
+template <class PP, class RS>
+__global__ void __launch_bounds__(TILE_THREADS) k_wave_tile(const DevParams P, const BufsT<RS> B, Ctl *ctl)
+{
+    typedef typename PP::R R;
+    if (!ctl->active) return;
+    extern __shared__ __align__(16) unsigned char smb[];
+    __shared__ double red8[TILE_THREADS / 32];
+    __shared__ bool last;
+    const StagedLayout L = StagedLayout::make(0, sizeof(R), 0);
+    const int64_t n = ctl->step;
+    const double t = ctl->t;
+    const SetV<RS> src = B.set[n & 1];
+    const double *zp = B.z[(n + 2) % 3];
+    const int64_t ntiles = (int64_t)((P.nx + T_I - 1) / T_I) * ((P.ny + T_J - 1) / T_J);
+    R smax = 0;
+    for (int64_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+        const R s = wave_tile<PP, RS>(P, src, zp, tile_coord(P, tile), smb, L, t);
+        smax = (s > smax) ? s : smax;
+    }
+    const double m = block_max((double)smax, red8);
+    if (threadIdx.x == 0) {
+        atomicMax(&ctl->smax_bits, (unsigned long long)__double_as_longlong(m));
+        __threadfence();
+        last = (atomicAdd(&ctl->wave_ticket, 1u) == gridDim.x - 1);
+    }
+    __syncthreads();
+    if (last && threadIdx.x == 0) wave_finalize(P, ctl);
+}
+
 /* ---------------------------------------------------------------- update */
 template <int MAXS, bool BUDGET>
 struct Acc2 {
@@ -895,117 +933,108 @@ __device__ __forceinline__ void stage_sample_tile(const DevParams &P, const SetV
     ctl->stageinterval += P.stageint;
 }
 
+/* Update of one tile: stages A (staging), B (faces), C (cells).  The whole
+ * block calls it. */
 template <class PP, class RS, int MAXS, bool BUDGET>
-__global__ void __launch_bounds__(TILE_THREADS, PP::kMinBlocks) k_update_tile(const DevParams P, const BufsT<RS> B, Ctl *ctl,
-                                                                  const double *__restrict__ rain, double *partials,
-                                                                  double *stage, double *saveflow)
+__device__ __forceinline__ void update_tile(const DevParams &P, const BufsT<RS> &B, int64_t n, double t, double dt,
+                                            double Rr, TileCoord tc, unsigned char *smb, const StagedLayout &L,
+                                            Acc2<MAXS, BUDGET> &acc)
 {
     typedef typename PP::R R;
-    if (!ctl->pending) return;
-    extern __shared__ __align__(16) unsigned char smb[];
-    const StagedLayout L = StagedLayout::make(P.S, sizeof(R), 1);
     const RealC<R> &K = kc<R>(P);
-    const int64_t n = ctl->step;
-    const double t = ctl->t, dt = ctl->dt;
     const SetV<RS> src = B.set[n & 1];
     const SetV<RS> dst = B.set[(n + 1) & 1];
     const double *zp = B.z[(n + 2) % 3], *zc = B.z[n % 3];
     double *zn = B.z[(n + 1) % 3];
     double inh = 0, inhv = 0, insed = 0;
     if (P.inflow) inflow_ghost(t, inh, inhv, insed);
-    const double Rr = P.storm ? 0.0 : rain_at(P, rain, t);
-    Acc2<MAXS, BUDGET> acc;
-    acc.rain = acc.out = acc.clamp = acc.bulk = acc.inf = acc.round = 0;
-#pragma unroll
-    for (int k = 0; k < (BUDGET ? MAXS : 1); k++) acc.det[k] = acc.sout[k] = acc.sround[k] = 0;
-    const int64_t ntiles = (int64_t)((P.nx + T_I - 1) / T_I) * ((P.ny + T_J - 1) / T_J);
     unsigned char *upb = smb + L.up;
     const R *su = reinterpret_cast<const R *>(smb + L.u), *sv = reinterpret_cast<const R *>(smb + L.v);
     const R *sg = reinterpret_cast<const R *>(smb + L.g), *sc = reinterpret_cast<const R *>(smb + L.c);
     R *sfx = reinterpret_cast<R *>(smb + L.fx), *sfy = reinterpret_cast<R *>(smb + L.fy);
-    for (int64_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
-        const TileCoord tc = tile_coord(P, tile);
-        stage_load<RS, 1>(P, src, zp, zc, B.ks, tc, smb, L);
-        __pipeline_wait_prior(0);
-        __syncthreads();
-        stage_derive<PP, RS, 1>(P, tc, smb, L, (R)inh, (R)inhv, (R)insed);
-        __syncthreads();
-        const RS *sh = staged_h<RS>(smb, L);
-        /* stage B: every face of the tile (SWEHR.c:1099-1230) */
-        for (int f = threadIdx.x; f < N_FX + N_FY; f += TILE_THREADS) {
-            R T0, T1, T2;
-            if (f < N_FX) {
-                const int fi = f / T_J, fj = f - fi * T_J;
-                const int gi = tc.i0 - 1 + fi, gj = tc.j0 + fj;
-                if (gj > P.ny || gi > P.nx) continue;
-                const int Lh = fi * H_J + fj + 1, Rh = Lh + H_J;
-                hllc_v<PP>((R)sh[fi * R_J + fj + 2], (R)sh[(fi + 1) * R_J + fj + 2], su[Lh], su[Rh], sv[Lh], sv[Rh],
-                           sg[Lh], sc[Lh], K.hfilm, T0, T1, T2);
-                R *F = sfx + 3 * f;
-                F[0] = T0; F[1] = T1; F[2] = T2;
-                upb[f] = (T0 > 0) ? 0 : 1;
-            } else {
-                const int f2 = f - N_FX;
-                const int fi = f2 / (T_J + 1), fj = f2 - fi * (T_J + 1);
-                const int gi = tc.i0 + fi, gj = tc.j0 - 1 + fj;
-                if (gi > P.nx || gj > P.ny) continue;
-                const int Lh = (fi + 1) * H_J + fj, Rh = Lh + 1;
-                hllc_v<PP>((R)sh[(fi + 1) * R_J + fj + 1], (R)sh[(fi + 1) * R_J + fj + 2], sv[Lh], sv[Rh], su[Lh],
-                           su[Rh], sg[Lh], sc[Lh], K.hfilm, T0, T1, T2);
-                R *F = sfy + 3 * f2;
-                F[0] = T0; F[1] = T2; F[2] = T1;
-                upb[f] = (T0 > 0) ? 0 : 1;
-            }
+    stage_load<RS, 1>(P, src, zp, zc, B.ks, tc, smb, L);
+    __pipeline_wait_prior(0);
+    __syncthreads();
+    stage_derive<PP, RS, 1>(P, tc, smb, L, (R)inh, (R)inhv, (R)insed);
+    __syncthreads();
+    const RS *sh = staged_h<RS>(smb, L);
+    /* stage B: every face of the tile (SWEHR.c:1099-1230) */
+    for (int f = threadIdx.x; f < N_FX + N_FY; f += TILE_THREADS) {
+        R T0, T1, T2;
+        if (f < N_FX) {
+            const int fi = f / T_J, fj = f - fi * T_J;
+            const int gi = tc.i0 - 1 + fi, gj = tc.j0 + fj;
+            if (gj > P.ny || gi > P.nx) continue;
+            const int Lh = fi * H_J + fj + 1, Rh = Lh + H_J;
+            hllc_v<PP>((R)sh[fi * R_J + fj + 2], (R)sh[(fi + 1) * R_J + fj + 2], su[Lh], su[Rh], sv[Lh], sv[Rh],
+                       sg[Lh], sc[Lh], K.hfilm, T0, T1, T2);
+            R *F = sfx + 3 * f;
+            F[0] = T0; F[1] = T1; F[2] = T2;
+            upb[f] = (T0 > 0) ? 0 : 1;
+        } else {
+            const int f2 = f - N_FX;
+            const int fi = f2 / (T_J + 1), fj = f2 - fi * (T_J + 1);
+            const int gi = tc.i0 + fi, gj = tc.j0 - 1 + fj;
+            if (gi > P.nx || gj > P.ny) continue;
+            const int Lh = (fi + 1) * H_J + fj, Rh = Lh + 1;
+            hllc_v<PP>((R)sh[(fi + 1) * R_J + fj + 1], (R)sh[(fi + 1) * R_J + fj + 2], sv[Lh], sv[Rh], su[Lh],
+                       su[Rh], sg[Lh], sc[Lh], K.hfilm, T0, T1, T2);
+            R *F = sfy + 3 * f2;
+            F[0] = T0; F[1] = T2; F[2] = T1;
+            upb[f] = (T0 > 0) ? 0 : 1;
         }
-        __syncthreads();
-        tile_cell<PP, RS, MAXS, BUDGET>(P, src, dst, zp, zc, zn, smb, L, tc, t, dt, Rr, acc);
-        __syncthreads();
     }
-    __shared__ bool last;
-    double *red = reinterpret_cast<double *>(smb + L.red);
-    if (BUDGET) {
-        double v[B_NTERMS];
-        v[B_RAIN] = acc.rain; v[B_OUT] = acc.out; v[B_CLAMP] = acc.clamp; v[B_BULK] = acc.bulk; v[B_INF] = acc.inf;
-        v[B_ROUND] = acc.round;
+    __syncthreads();
+    tile_cell<PP, RS, MAXS, BUDGET>(P, src, dst, zp, zc, zn, smb, L, tc, t, dt, Rr, acc);
+    __syncthreads();
+}
+
+/* Block sum of the budget accumulators into red[B_NTERMS] (thread 0 holds
+ * the block's totals afterwards); fixed order, so deterministic. */
+template <int MAXS, bool BUDGET>
+__device__ __forceinline__ void budget_block_sum(const Acc2<MAXS, BUDGET> &acc, double *red)
+{
+    double v[B_NTERMS];
+    v[B_RAIN] = acc.rain; v[B_OUT] = acc.out; v[B_CLAMP] = acc.clamp; v[B_BULK] = acc.bulk; v[B_INF] = acc.inf;
+    v[B_ROUND] = acc.round;
 #pragma unroll
-        for (int k = 0; k < 16; k++) {
-            v[B_DET + k] = (k < MAXS) ? acc.det[k < MAXS ? k : 0] : 0.0;
-            v[B_SOUT + k] = (k < MAXS) ? acc.sout[k < MAXS ? k : 0] : 0.0;
-            v[B_SROUND + k] = (k < MAXS) ? acc.sround[k < MAXS ? k : 0] : 0.0;
-        }
+    for (int k = 0; k < 16; k++) {
+        v[B_DET + k] = (k < MAXS) ? acc.det[k < MAXS ? k : 0] : 0.0;
+        v[B_SOUT + k] = (k < MAXS) ? acc.sout[k < MAXS ? k : 0] : 0.0;
+        v[B_SROUND + k] = (k < MAXS) ? acc.sround[k < MAXS ? k : 0] : 0.0;
+    }
 #pragma unroll
+    for (int m = 0; m < B_NTERMS; m++) {
+        const double s = warp_sum(v[m]);
+        if ((threadIdx.x & 31) == 0) red[(threadIdx.x >> 5) * B_NTERMS + m] = s;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0)
         for (int m = 0; m < B_NTERMS; m++) {
-            const double s = warp_sum(v[m]);
-            if ((threadIdx.x & 31) == 0) red[(threadIdx.x >> 5) * B_NTERMS + m] = s;
+            double s = 0;
+            for (int w = 0; w < TILE_THREADS / 32; w++) s += red[w * B_NTERMS + m];
+            red[m] = s;
         }
-    }
-    __threadfence();
     __syncthreads();
-    if (threadIdx.x == 0) {
-        if (BUDGET) {
-            for (int m = 0; m < B_NTERMS; m++) {
-                double s = 0;
-                for (int w = 0; w < TILE_THREADS / 32; w++) s += red[w * B_NTERMS + m];
-                partials[(int64_t)blockIdx.x * B_NTERMS + m] = s;
-            }
-        }
-        __threadfence();
-        const unsigned tk = atomicAdd(&ctl->update_ticket, 1u);
-        last = (tk == gridDim.x - 1);
-    }
-    __syncthreads();
-    if (!last) return;
+}
+
+template <int MAXS, bool BUDGET>
+__device__ __forceinline__ void acc_zero(Acc2<MAXS, BUDGET> &acc)
+{
+    acc.rain = acc.out = acc.clamp = acc.bulk = acc.inf = acc.round = 0;
+#pragma unroll
+    for (int k = 0; k < (BUDGET ? MAXS : 1); k++) acc.det[k] = acc.sout[k] = acc.sround[k] = 0;
+}
+
+/* End of a step once every cell is written (whole block): time, step
+ * counter, stage row (SWEHR.c:1591-1676), stop conditions. */
+template <class PP, class RS>
+__device__ __forceinline__ void update_finalize(const DevParams &P, const SetV<RS> &dst, Ctl *ctl, double *stage,
+                                                double *saveflow, unsigned char *smb)
+{
     __threadfence();
-    if (BUDGET && threadIdx.x < B_NTERMS) {
-        double hi = 0, lo = 0;
-        for (unsigned b = 0; b < gridDim.x; b++)
-            dd_add(hi, lo, ((volatile double *)partials)[(int64_t)b * B_NTERMS + threadIdx.x]);
-        double Hh = ctl->budget_hi[threadIdx.x], Ll = ctl->budget_lo[threadIdx.x];
-        dd_add(Hh, Ll, hi);
-        Ll += lo;
-        ctl->budget_hi[threadIdx.x] = Hh;
-        ctl->budget_lo[threadIdx.x] = Ll;
-    }
+    const int64_t n = ctl->step;
+    const double t = ctl->t, dt = ctl->dt;
     const double tnew = (ctl->cfl ? 2 * P.tend : t) + dt;
     const bool stage_due = tnew > ctl->stageinterval && ctl->stagecnt < ctl->stagecap;
     __syncthreads();
@@ -1021,6 +1050,153 @@ __global__ void __launch_bounds__(TILE_THREADS, PP::kMinBlocks) k_update_tile(co
         if (ctl->cfl || !(dt > 0) || !(tnew < P.tend) || !(tnew < ctl->t_stop) || n + 1 >= ctl->max_step)
             ctl->active = 0;
         ctl->launches += 2;
+    }
+}
+
+__device__ __forceinline__ void budget_fold(Ctl *ctl, int m, double hi, double lo)
+{
+    double Hh = ctl->budget_hi[m], Ll = ctl->budget_lo[m];
+    dd_add(Hh, Ll, hi);
+    Ll += lo;
+    ctl->budget_hi[m] = Hh;
+    ctl->budget_lo[m] = Ll;
+}
+
+template <class PP, class RS, int MAXS, bool BUDGET>
+__global__ void __launch_bounds__(TILE_THREADS, PP::kMinBlocks) k_update_tile(const DevParams P, const BufsT<RS> B, Ctl *ctl,
+                                                                  const double *__restrict__ rain, double *partials,
+                                                                  double *stage, double *saveflow)
+{
+    typedef typename PP::R R;
+    if (!ctl->pending) return;
+    extern __shared__ __align__(16) unsigned char smb[];
+    __shared__ bool last;
+    const StagedLayout L = StagedLayout::make(P.S, sizeof(R), 1);
+    const int64_t n = ctl->step;
+    const double t = ctl->t, dt = ctl->dt;
+    const double Rr = P.storm ? 0.0 : rain_at(P, rain, t);
+    Acc2<MAXS, BUDGET> acc;
+    acc_zero(acc);
+    const int64_t ntiles = (int64_t)((P.nx + T_I - 1) / T_I) * ((P.ny + T_J - 1) / T_J);
+    for (int64_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x)
+        update_tile<PP, RS, MAXS, BUDGET>(P, B, n, t, dt, Rr, tile_coord(P, tile), smb, L, acc);
+    double *red = reinterpret_cast<double *>(smb + L.red);
+    if (BUDGET) budget_block_sum(acc, red);
+    __threadfence();
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        if (BUDGET)
+            for (int m = 0; m < B_NTERMS; m++) partials[(int64_t)blockIdx.x * B_NTERMS + m] = red[m];
+        __threadfence();
+        last = (atomicAdd(&ctl->update_ticket, 1u) == gridDim.x - 1);
+    }
+    __syncthreads();
+    if (!last) return;
+    __threadfence();
+    if (BUDGET && threadIdx.x < B_NTERMS) {
+        double hi = 0, lo = 0;
+        for (unsigned b = 0; b < gridDim.x; b++)
+            dd_add(hi, lo, ((volatile double *)partials)[(int64_t)b * B_NTERMS + threadIdx.x]);
+        budget_fold(ctl, threadIdx.x, hi, lo);
+    }
+    update_finalize<PP, RS>(P, B.set[(n + 1) & 1], ctl, stage, saveflow, smb);
+}
+
+/* ------------------------------------------------------------- batched ---
+ * Many independent scenarios of uneven sizes stepped by one launch of each
+ * kernel.  The tiles of all scenarios form one list (scenario s owns tiles
+ * [tile0, tile0 + ntiles)); a persistent grid walks it.  Each scenario keeps
+ * its own control block, dt, t and stage rows: the block that completes a
+ * scenario's last tile finalizes that scenario.  Finished scenarios' tiles
+ * are skipped with one load.  Per-cell arithmetic is the single-domain
+ * arithmetic, so every scenario's result is identical alone or in a batch.
+ * Budget sums of a batched step are block partials added with atomics
+ * (order-dependent rounding of the budget terms only). */
+template <class RS>
+__device__ __forceinline__ int scen_of(const ScenDesc<RS> *tab, int nscen, int64_t g)
+{
+    int lo = 0, hi = nscen - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (tab[mid].tile0 <= g) lo = mid; else hi = mid - 1;
+    }
+    return lo;
+}
+
+template <class PP, class RS>
+__global__ void __launch_bounds__(TILE_THREADS) k_wave_batch(const BatchHdr<RS> *__restrict__ hdr)
+{
+    typedef typename PP::R R;
+    extern __shared__ __align__(16) unsigned char smb[];
+    __shared__ double red8[TILE_THREADS / 32];
+    const StagedLayout L = StagedLayout::make(0, sizeof(R), 0);
+    const ScenDesc<RS> *tab = hdr->tab;
+    const int nscen = hdr->nscen;
+    const int64_t total = hdr->total_tiles;
+    for (int64_t g = blockIdx.x; g < total; g += gridDim.x) {
+        const ScenDesc<RS> &D = tab[scen_of(tab, nscen, g)];
+        Ctl *ctl = D.ctl;
+        if (!ctl->active) continue;                              /* uniform across the block */
+        const int64_t n = ctl->step;
+        const R s = wave_tile<PP, RS>(D.P, D.B.set[n & 1], D.B.z[(n + 2) % 3], tile_coord(D.P, g - D.tile0), smb, L,
+                                      ctl->t);
+        const double m = block_max((double)s, red8);
+        if (threadIdx.x == 0) {
+            atomicMax(&ctl->smax_bits, (unsigned long long)__double_as_longlong(m));
+            __threadfence();
+            if (atomicAdd(&ctl->wave_ticket, 1u) == (unsigned)(D.ntiles - 1)) wave_finalize(D.P, ctl);
+        }
+        __syncthreads();
+    }
+}
+
+template <class PP, class RS, int MAXS, bool BUDGET>
+__global__ void __launch_bounds__(TILE_THREADS, PP::kMinBlocks) k_update_batch(const BatchHdr<RS> *__restrict__ hdr)
+{
+    typedef typename PP::R R;
+    extern __shared__ __align__(16) unsigned char smb[];
+    __shared__ bool last;
+    const ScenDesc<RS> *tab = hdr->tab;
+    const int nscen = hdr->nscen;
+    const int64_t total = hdr->total_tiles;
+    for (int64_t g = blockIdx.x; g < total; g += gridDim.x) {
+        const ScenDesc<RS> &D = tab[scen_of(tab, nscen, g)];
+        Ctl *ctl = D.ctl;
+        if (!ctl->pending) continue;                             /* uniform across the block */
+        const StagedLayout L = StagedLayout::make(D.P.S, sizeof(R), 1);
+        const int64_t n = ctl->step;
+        const double t = ctl->t, dt = ctl->dt;
+        const double Rr = D.P.storm ? 0.0 : rain_at(D.P, D.rain, t);
+        Acc2<MAXS, BUDGET> acc;
+        acc_zero(acc);
+        update_tile<PP, RS, MAXS, BUDGET>(D.P, D.B, n, t, dt, Rr, tile_coord(D.P, g - D.tile0), smb, L, acc);
+        double *red = reinterpret_cast<double *>(smb + L.red);
+        const bool bud = BUDGET && D.P.budget;
+        if (bud) budget_block_sum(acc, red);
+        __threadfence();
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            if (bud)
+                for (int m = 0; m < B_NTERMS; m++) atomicAdd(&ctl->budget_step[m], red[m]);
+            __threadfence();
+            last = (atomicAdd(&ctl->update_ticket, 1u) == (unsigned)(D.ntiles - 1));
+        }
+        __syncthreads();
+        if (last) {
+            __threadfence();
+            if (bud && threadIdx.x < B_NTERMS) {
+                const double v = atomicAdd(&ctl->budget_step[threadIdx.x], 0.0);
+                ctl->budget_step[threadIdx.x] = 0.0;
+                budget_fold(ctl, threadIdx.x, v, 0.0);
+            }
+            update_finalize<PP, RS>(D.P, D.B.set[(n + 1) & 1], ctl, D.stage, D.saveflow, smb);
+            if (threadIdx.x == 0) {
+                ScenSummary *q = D.sum;
+                q->t = ctl->t; q->dt = ctl->dt; q->courant = ctl->courant; q->step = ctl->step;
+                q->status = ctl->status; q->active = ctl->active;
+            }
+        }
+        __syncthreads();
     }
 }
 

@@ -10,8 +10,8 @@ import os
 
 import numpy as np
 
-from .params import (SwehrParams, SwehrInputs, SwehrProgress, SwehrBudget, FIELD_NAMES, PER_CLASS_FIELDS,
-                     STATUS, FP64)
+from .params import (SwehrParams, SwehrInputs, SwehrProgress, SwehrBudget, SwehrPoolStats, FIELD_NAMES,
+                     PER_CLASS_FIELDS, STATUS, STATUS_BUSY, FP64)
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "libswehr.so")
@@ -58,6 +58,23 @@ def load() -> C.CDLL:
     L.swehr_destroy.argtypes = [vp]
     L.swehr_cfl_noalloc.restype = i32
     L.swehr_cfl_noalloc.argtypes = [vp, vp, vp, vp, vp, i64, dbl, vp, vp]
+    L.swehr_pool_create.restype = i32
+    L.swehr_pool_create.argtypes = [i32, i32, i32, C.c_size_t, i32, C.POINTER(vp)]
+    L.swehr_pool_submit.restype = i32
+    L.swehr_pool_submit.argtypes = [vp, vp, vp, i64, C.POINTER(i32)]
+    L.swehr_pool_run.restype = i32
+    L.swehr_pool_run.argtypes = [vp, i64, vp]
+    L.swehr_pool_tune.restype = i32
+    L.swehr_pool_tune.argtypes = [vp, i64, vp]
+    L.swehr_pool_poll.restype = i32
+    L.swehr_pool_poll.argtypes = [vp, i32, vp]
+    L.swehr_pool_scenario.restype = i32
+    L.swehr_pool_scenario.argtypes = [vp, i32, C.POINTER(vp)]
+    L.swehr_pool_release.restype = i32
+    L.swehr_pool_release.argtypes = [vp, i32]
+    L.swehr_pool_stats_get.restype = i32
+    L.swehr_pool_stats_get.argtypes = [vp, vp]
+    L.swehr_pool_destroy.argtypes = [vp]
     if L.swehr_params_size() != C.sizeof(SwehrParams):
         raise ImportError(f"swehr_params size mismatch: C {L.swehr_params_size()} vs ctypes {C.sizeof(SwehrParams)}")
     _lib = L
@@ -68,12 +85,11 @@ def _dptr(a):
     return a.ctypes.data_as(C.POINTER(C.c_double))
 
 
-class Simulation:
-    """One SWEHR run on the GPU through the C ABI."""
+class CaseInputs:
+    """A case's parameters and input arrays held in C layout (kept alive as
+    long as the C side may read them)."""
 
-    def __init__(self, case, precision: int = FP64, budget: bool = False):
-        self.L = load()
-        self.case = case
+    def __init__(self, case, budget: bool = False):
         self.params = case.make_params()
         if budget:
             self.params.budget = 1
@@ -82,10 +98,62 @@ class Simulation:
         self._ds = np.ascontiguousarray(case.ds, dtype=np.float64)
         self._pf = np.ascontiguousarray(case.pfrac, dtype=np.float64)
         self._ks = None if case.ks is None else np.ascontiguousarray(case.ks, dtype=np.float64)
-        inp = SwehrInputs(_dptr(self._topo), _dptr(self._rain), _dptr(self._ds), _dptr(self._pf),
-                          _dptr(self._ks) if self._ks is not None else None)
+        self.inputs = SwehrInputs(_dptr(self._topo), _dptr(self._rain), _dptr(self._ds), _dptr(self._pf),
+                                  _dptr(self._ks) if self._ks is not None else None)
+
+    @property
+    def host_bytes(self) -> int:
+        n = self._topo.nbytes + self._rain.nbytes + self._ds.nbytes + self._pf.nbytes
+        return n + (self._ks.nbytes if self._ks is not None else 0)
+
+
+class _Reader:
+    """Field, series and budget reads of one context handle."""
+
+    def _check(self, st):
+        if st != 0:
+            raise SwehrError(st, self.L.swehr_last_error().decode())
+
+    def field(self, name: str, k: int = 0) -> np.ndarray:
+        out = np.empty((self.case.nx, self.case.ny))
+        self._check(self.L.swehr_read_field(self.ctx, FIELD_NAMES[name], k, out.ctypes.data))
+        return out
+
+    def fields(self, names=None) -> dict:
+        if names is None:
+            names = ("h", "hu", "hv", "z", "vinf", "totm", "dep", "totsed", "maxvel", "maxdepth", "vel",
+                     "U", "M", "sed")
+        d = {}
+        for n in names:
+            if FIELD_NAMES[n] in PER_CLASS_FIELDS:
+                d[n] = np.stack([self.field(n, k) for k in range(1, self.case.sclass + 1)])
+            else:
+                d[n] = self.field(n)
+        return d
+
+    def series(self, max_rows: int = 200000):
+        st = np.empty((max_rows, 24))
+        sf = np.empty((max_rows, 18))
+        rows = C.c_int64()
+        self._check(self.L.swehr_read_series(self.ctx, st.ctypes.data, sf.ctypes.data, max_rows, C.byref(rows)))
+        return st[: rows.value].copy(), sf[: rows.value].copy()
+
+    def budget(self) -> SwehrBudget:
+        b = SwehrBudget()
+        self._check(self.L.swehr_get_budget(self.ctx, C.byref(b)))
+        return b
+
+
+class Simulation(_Reader):
+    """One SWEHR run on the GPU through the C ABI."""
+
+    def __init__(self, case, precision: int = FP64, budget: bool = False):
+        self.L = load()
+        self.case = case
+        self._in = CaseInputs(case, budget)
+        self.params = self._in.params
         self.ctx = C.c_void_p()
-        st = self.L.swehr_create(C.byref(self.params), C.byref(inp), precision, C.byref(self.ctx))
+        st = self.L.swehr_create(C.byref(self.params), C.byref(self._in.inputs), precision, C.byref(self.ctx))
         if st != 0:
             raise SwehrError(st, self.L.swehr_last_error().decode())
 
@@ -100,46 +168,106 @@ class Simulation:
     def set_timing(self, on: bool):
         self.L.swehr_set_timing(self.ctx, 1 if on else 0)
 
-    def field(self, name: str, k: int = 0) -> np.ndarray:
-        out = np.empty((self.case.nx, self.case.ny))
-        st = self.L.swehr_read_field(self.ctx, FIELD_NAMES[name], k, out.ctypes.data)
-        if st != 0:
-            raise SwehrError(st, self.L.swehr_last_error().decode())
-        return out
-
-    def fields(self) -> dict:
-        names = ("h", "hu", "hv", "z", "vinf", "totm", "dep", "totsed", "maxvel", "maxdepth", "vel")
-        d = {n: self.field(n) for n in names}
-        for g in ("U", "M", "sed"):
-            d[g] = np.stack([self.field(g, k) for k in range(1, self.case.sclass + 1)])
-        return d
-
     def write_field(self, name: str, arr: np.ndarray, k: int = 0):
         a = np.ascontiguousarray(arr, dtype=np.float64)
         st = self.L.swehr_write_field(self.ctx, FIELD_NAMES[name], k, a.ctypes.data)
         if st != 0:
             raise SwehrError(st, self.L.swehr_last_error().decode())
 
-    def series(self, max_rows: int = 200000):
-        st = np.empty((max_rows, 24))
-        sf = np.empty((max_rows, 18))
-        rows = C.c_int64()
-        r = self.L.swehr_read_series(self.ctx, st.ctypes.data, sf.ctypes.data, max_rows, C.byref(rows))
-        if r != 0:
-            raise SwehrError(r, self.L.swehr_last_error().decode())
-        return st[: rows.value].copy(), sf[: rows.value].copy()
-
-    def budget(self) -> SwehrBudget:
-        b = SwehrBudget()
-        st = self.L.swehr_get_budget(self.ctx, C.byref(b))
-        if st != 0:
-            raise SwehrError(st, self.L.swehr_last_error().decode())
-        return b
-
     def close(self):
         if getattr(self, "ctx", None):
             self.L.swehr_destroy(self.ctx)
             self.ctx = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class PoolScenario(_Reader):
+    """A scenario resident in a Pool (reads only; the pool steps it)."""
+
+    def __init__(self, pool, sid: int, case, inputs: CaseInputs):
+        self.L = pool.L
+        self.pool = pool
+        self.id = sid
+        self.case = case
+        self._in = inputs
+        self.ctx = C.c_void_p()
+        self._check(self.L.swehr_pool_scenario(pool.handle, sid, C.byref(self.ctx)))
+
+    def progress(self) -> SwehrProgress:
+        pr = SwehrProgress()
+        self._check(self.L.swehr_pool_poll(self.pool.handle, self.id, C.byref(pr)))
+        return pr
+
+
+class Pool:
+    """Many scenarios stepped by shared persistent launches (swehr_pool_*)."""
+
+    def __init__(self, precision: int = FP64, max_classes: int = 16, budget: bool = False, hbm_limit: int = 0,
+                 max_scenarios: int = 4096):
+        self.L = load()
+        self.budget_on = budget
+        self.handle = C.c_void_p()
+        st = self.L.swehr_pool_create(precision, max_classes, 1 if budget else 0, hbm_limit, max_scenarios,
+                                      C.byref(self.handle))
+        if st != 0:
+            raise SwehrError(st, self.L.swehr_last_error().decode())
+        self.scenarios = {}
+
+    def submit(self, case, max_steps: int = -1, budget: bool = False):
+        """The new PoolScenario, or None when the pool is full right now."""
+        inp = CaseInputs(case, budget)
+        sid = C.c_int()
+        st = self.L.swehr_pool_submit(self.handle, C.byref(inp.params), C.byref(inp.inputs), max_steps,
+                                      C.byref(sid))
+        if st == STATUS_BUSY:
+            return None
+        if st != 0:
+            raise SwehrError(st, self.L.swehr_last_error().decode())
+        sc = PoolScenario(self, sid.value, case, inp)
+        self.scenarios[sid.value] = sc
+        return sc
+
+    def run(self, steps: int = -1) -> SwehrPoolStats:
+        s = SwehrPoolStats()
+        st = self.L.swehr_pool_run(self.handle, steps, C.byref(s))
+        if st != 0:
+            raise SwehrError(st, self.L.swehr_last_error().decode())
+        return s
+
+    def tune(self, steps_per_trial: int = 8) -> SwehrPoolStats:
+        s = SwehrPoolStats()
+        st = self.L.swehr_pool_tune(self.handle, steps_per_trial, C.byref(s))
+        if st != 0:
+            raise SwehrError(st, self.L.swehr_last_error().decode())
+        return s
+
+    def stats(self) -> SwehrPoolStats:
+        s = SwehrPoolStats()
+        self.L.swehr_pool_stats_get(self.handle, C.byref(s))
+        return s
+
+    def release(self, sc):
+        st = self.L.swehr_pool_release(self.handle, sc.id)
+        if st != 0:
+            raise SwehrError(st, self.L.swehr_last_error().decode())
+        self.scenarios.pop(sc.id, None)
+
+    def close(self):
+        if getattr(self, "handle", None):
+            self.L.swehr_pool_destroy(self.handle)
+            self.handle = None
+            self.scenarios = {}
 
     def __enter__(self):
         return self

@@ -79,6 +79,17 @@ class SwehrBudget(C.Structure):
     ]
 
 
+class SwehrPoolStats(C.Structure):
+    _fields_ = [
+        ("resident", C.c_int32), ("running", C.c_int32), ("finished_now", C.c_int32), ("tuned", C.c_int32),
+        ("pool_steps", C.c_int64), ("cell_steps", C.c_int64), ("device_ms", C.c_double),
+        ("hbm_used", C.c_size_t), ("hbm_limit", C.c_size_t),
+        ("grid_wave", C.c_int32), ("grid_update", C.c_int32),
+    ]
+
+
+STATUS_BUSY = 8
+
 # Reference defaults: SWEHR.c:490-494 (friction/splash exponents), 617-650
 # (boundaries, stepping, physical constants), 236-246 (soil), 709-715 (points).
 REFERENCE_DEFAULTS = dict(

@@ -109,3 +109,25 @@ def test_footprint_scales_with_cells_and_classes():
     b = L.swehr_footprint_bytes(8192, 8192, 10, 0)
     assert 6e9 < a < 8e9
     assert b > 3.5 * a
+
+
+def test_pool_entry_points_check_arguments_without_device():
+    L = swlib.load()
+    h = C.c_void_p()
+    assert L.swehr_pool_create(7, 4, 0, 0, 8, C.byref(h)) == 5          # unknown precision
+    assert L.swehr_pool_create(0, 0, 0, 0, 8, C.byref(h)) == 5          # max_classes
+    assert L.swehr_pool_create(0, 4, 0, 0, 0, C.byref(h)) == 5          # max_scenarios
+    assert L.swehr_pool_run(None, 1, None) == 5
+    assert L.swehr_pool_release(None, 1) == 5
+    L.swehr_pool_destroy(None)
+    if not _has_device():
+        assert L.swehr_pool_create(0, 4, 0, 0, 8, C.byref(h)) == 7      # no device
+        assert not h.value
+
+
+def _has_device():
+    try:
+        import torch
+        return torch.cuda.is_available()
+    except Exception:
+        return False
