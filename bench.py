@@ -172,6 +172,93 @@ def reference_arm(args, rank: int):
     print(json.dumps(line))
 
 
+def ensemble_leg(args):
+    """The batched ensemble: scenarios with sides log-uniform in 64..1024
+    cells (dx = 1 m, per-scenario fractal seeds, rain U(20,150) mm/h, Manning
+    n U(0.02,0.08), 7 classes) resident in one pool and stepped by shared
+    persistent launches, in the mixed and in the plain FP64 form; each form's
+    launch shape picked by the pool's tuner first.  Every scenario is capped
+    at the same step count, so after the timed steps both pools hold the
+    same steps of every scenario and a subset is compared field by field
+    (mixed vs FP64, beside FP64 on FP32-rounded inputs: the envelope)."""
+    from swehr_b200.accuracy import rel_linf, quantized_case
+    from swehr_b200 import workloads as W
+    from swehr_b200.lib import Pool, Simulation
+    from swehr_b200.params import FP64, MIXED
+    cases = W.ensemble(args.ens_count)
+    cells = sum(c.cells() for c in cases)
+    cap = 64 + args.ens_warmup + args.ens_steps
+    subset = list(range(0, len(cases), max(1, len(cases) // 8)))[:8]
+    names = ("h", "totsed", "sed")
+    out, keep = {}, {}
+    for label, prec in (("fp64", FP64), ("mixed", MIXED)):
+        with Pool(precision=prec, max_classes=8, max_scenarios=len(cases) + 1) as pool:
+            t0 = time.perf_counter()
+            scs = [pool.submit(c, max_steps=cap) for c in cases]
+            if any(s is None for s in scs):
+                raise RuntimeError("ensemble does not fit the pool")
+            upload_s = time.perf_counter() - t0
+            tu = pool.tune(4)
+            pool.run(args.ens_warmup)
+            st = pool.run(args.ens_steps)
+            v = st.cell_steps / (st.device_ms / 1e3)
+            pool.run(-1)
+            keep[label] = [scs[k].fields(names) for k in subset]
+            out[label] = {"value": v, "unit": "cell-steps/s", "pool_steps": int(st.pool_steps),
+                          "device_ms": st.device_ms, "ms_per_pool_step": st.device_ms / max(st.pool_steps, 1),
+                          "grid_wave": int(tu.grid_wave), "grid_update": int(tu.grid_update),
+                          "upload_s": upload_s, "hbm_bytes": int(st.hbm_used)}
+    # envelope: FP64 on the subset's inputs rounded to FP32
+    env = []
+    with Pool(precision=FP64, max_classes=8, max_scenarios=len(subset) + 1) as pool:
+        scs = [pool.submit(quantized_case(cases[k]), max_steps=cap) for k in subset]
+        pool.run(-1)
+        env = [s.fields(names) for s in scs]
+    err = {n: 0.0 for n in names}
+    envm = {n: 0.0 for n in names}
+    for a, b, q in zip(keep["mixed"], keep["fp64"], env):
+        for n in names:
+            err[n] = max(err[n], rel_linf(a[n], b[n]))
+            envm[n] = max(envm[n], rel_linf(q[n], b[n]))
+    # the same scenarios one at a time through the single-domain path (FP64)
+    t_dev, cs = 0.0, 0
+    for c in cases[:: max(1, len(cases) // 32)]:
+        with Simulation(c) as sim:
+            sim.advance(max_steps=3)
+            pr = sim.advance(max_steps=args.ens_solo_steps)
+            t_dev += pr.device_ms
+            cs += c.cells() * pr.steps_this_call
+    solo = cs / (t_dev / 1e3)
+    return {"workload": f"{len(cases)} scenarios, sides log-uniform 64..1024 (seed 2), {cells} cells, 7 classes",
+            "scenarios": len(cases), "cells": cells, "steps_per_scenario": cap,
+            "batched_mixed": out["mixed"], "batched_fp64": out["fp64"],
+            "solo_fp64": {"value": solo, "unit": "cell-steps/s",
+                          "sample": f"every {max(1, len(cases) // 32)}th scenario alone, "
+                                    f"{args.ens_solo_steps} steps each"},
+            "mixed_over_batched_fp64": out["mixed"]["value"] / out["fp64"]["value"],
+            "mixed_over_solo_fp64": out["mixed"]["value"] / solo,
+            "error_vs_fp64": {"scenarios": [int(k) for k in subset], "rel_linf": err,
+                              "fp32_input_envelope": envm}}
+
+
+def serving_leg(args):
+    """A Poisson request stream through the continuous-batching server."""
+    from swehr_b200 import serving as SV
+    from swehr_b200.params import MIXED
+    reqs = SV.poisson_stream(rate=args.serve_rate, duration=args.serve_duration, seed=3, side_min=32,
+                             side_max=args.serve_side_max, hyeto_steps=(1, args.serve_hyeto_max))
+    SV.prepare(reqs)
+    srv = SV.Server(precision=MIXED, hbm_limit=150 * 10 ** 9, max_classes=16, chunk_steps=16)
+    rep = srv.serve(reqs, time_limit=args.serve_duration + args.serve_drain)
+    d = rep.summary()
+    d.update({"workload": f"Poisson {args.serve_rate}/s for {args.serve_duration} s (seed 3), hillslope or "
+                          f"fractal squares, side log-uniform 32..{args.serve_side_max}, 5-10 classes, "
+                          f"1-{args.serve_hyeto_max} hyetograph steps of 10-60 s at 0-150 mm/h, dx=1 m, "
+                          "mixed form, 150 GB HBM admission limit",
+              "latency": "arrival -> result fields (h, totsed) on the host"})
+    return d
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -183,6 +270,17 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-mixed", action="store_true")
+    ap.add_argument("--no-ensemble", action="store_true")
+    ap.add_argument("--no-serving", action="store_true")
+    ap.add_argument("--ens-count", type=int, default=256)
+    ap.add_argument("--ens-warmup", type=int, default=8)
+    ap.add_argument("--ens-steps", type=int, default=200)
+    ap.add_argument("--ens-solo-steps", type=int, default=50)
+    ap.add_argument("--serve-rate", type=float, default=50.0)
+    ap.add_argument("--serve-duration", type=float, default=10.0)
+    ap.add_argument("--serve-drain", type=float, default=50.0)
+    ap.add_argument("--serve-side-max", type=int, default=512)
+    ap.add_argument("--serve-hyeto-max", type=int, default=3)
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
@@ -299,6 +397,18 @@ def main():
             cpu = {"value": None, "unit": "cell-steps/s", "cores": host_threads(), "kind": "reference",
                    "sample": f"unavailable: {e}"}
 
+    ensemble = serving = None
+    if rank == 0 and world == 1 and not args.no_ensemble:
+        try:
+            ensemble = ensemble_leg(args)
+        except Exception as e:  # noqa: BLE001
+            ensemble = {"error": repr(e)}
+    if rank == 0 and world == 1 and not args.no_serving:
+        try:
+            serving = serving_leg(args)
+        except Exception as e:  # noqa: BLE001
+            serving = {"error": repr(e)}
+
     if rank == 0:
         peak, peak_kind = hbm_peak()
         B = algo_bytes_f64(S)
@@ -328,6 +438,8 @@ def main():
             "cpu_baseline": cpu,
             "e2e": e2e,
             "mixed_form": mixed,
+            "batched_ensemble": ensemble,
+            "serving": serving,
             "clocks": clk,
             "gpu_launches": int(pr.kernel_launches),
             "impl": "swehr",

@@ -87,6 +87,7 @@ struct Ctl {
     int64_t launches;
     double budget_hi[64], budget_lo[64];   /* running compensated budget sums */
     double budget_step[64];                 /* this step's partials in batched mode */
+    double rain_now;                        /* batched mode: uniform rain rate of the pending step */
     double sed0[16];
 };
 

@@ -42,6 +42,7 @@ struct BatchHdr {
     const ScenDesc<RS> *tab;
     int32_t nscen, pad;
     int64_t total_tiles;
+    const int32_t *tile_scen;        /* scenario of each tile of the list */
 };
 
 /* the batched kernels of one form (both take one argument: the header) */
@@ -51,6 +52,10 @@ struct BatchConfig {
     int occ_wave = 1, occ_update = 1;   /* resident blocks per SM */
     int threads = 0;                    /* threads per block */
     int tile_i = 0, tile_j = 0;         /* cells per tile */
+    /* update kernel: dynamic shared memory and resident blocks per SM when
+     * the largest class count among the scenarios is S (index S = 0..16) */
+    size_t smem_update_s[17] = {};
+    int occ_update_s[17] = {};
 };
 
 int configure_batch_f64(int max_classes, bool budget, BatchConfig &cfg);

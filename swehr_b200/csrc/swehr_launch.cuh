@@ -75,6 +75,14 @@ struct FormLauncher {
         if (e != cudaSuccess) return (int)e;
         if (cfg.occ_update < 1) cfg.occ_update = 1;
         if (cfg.occ_wave < 1) cfg.occ_wave = 1;
+        for (int S = 0; S <= 16; S++) {
+            const int Sc = S < 1 ? 1 : (S > max_classes ? max_classes : S);
+            cfg.smem_update_s[S] = update_smem(Sc);
+            int o = 0;
+            e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o, fu, TILE_THREADS, cfg.smem_update_s[S]);
+            if (e != cudaSuccess) return (int)e;
+            cfg.occ_update_s[S] = o < 1 ? 1 : o;
+        }
         cfg.fn_update = fu;
         cfg.fn_wave = fw;
         cfg.smem_update = su;

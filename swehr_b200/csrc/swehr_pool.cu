@@ -52,6 +52,9 @@ struct swehr_pool {
     size_t hbm_limit = 0, hbm_used = 0;
     BatchConfig cfg;
     int grid_wave = 0, grid_update = 0, tuned = 0;
+    int kw_sel = 0, ku_sel = 0;          /* tuned blocks per SM (0: occupancy) */
+    int max_s = 1;                       /* largest class count running */
+    size_t smem_update = 0;              /* update kernel's dynamic shared memory now */
     cudaStream_t stream = nullptr;
     cudaGraphExec_t graph = nullptr;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
@@ -60,6 +63,8 @@ struct swehr_pool {
     char *d_tab = nullptr, *h_tab = nullptr;
     size_t desc_bytes = 0;
     ScenSummary *d_sum = nullptr, *h_sum = nullptr;
+    int32_t *d_map = nullptr, *h_map = nullptr;   /* tile -> scenario */
+    int64_t map_cap = 0;
     std::vector<PoolScen> scen;
     std::vector<int> free_slots;
     int next_id = 1;
@@ -89,6 +94,8 @@ static void pool_free(swehr_pool *pl)
     if (pl->d_hdr) cudaFree(pl->d_hdr);
     if (pl->d_tab) cudaFree(pl->d_tab);
     if (pl->d_sum) cudaFree(pl->d_sum);
+    if (pl->d_map) cudaFree(pl->d_map);
+    if (pl->h_map) cudaFreeHost(pl->h_map);
     if (pl->h_hdr) cudaFreeHost(pl->h_hdr);
     if (pl->h_tab) cudaFreeHost(pl->h_tab);
     if (pl->h_sum) cudaFreeHost(pl->h_sum);
@@ -113,13 +120,16 @@ static void fill_desc(const PoolScen &s, const BufsT<RS> &B, ScenSummary *d_sum,
     memcpy(out, &d, sizeof d);
 }
 
+static void apply_shape(swehr_pool *pl);
+
 /* write the running scenarios into the device table and header */
 static int rebuild_table(swehr_pool *pl)
 {
-    int k = 0;
+    int k = 0, max_s = 1;
     int64_t tile0 = 0, cells = 0;
     for (auto &s : pl->scen) {
         if (!s.running) continue;
+        max_s = std::max(max_s, (int)s.ctx->P.S);
         char *slot = pl->h_tab + (size_t)k * pl->desc_bytes;
         if (pl->precision == SWEHR_MIXED)
             fill_desc<float>(s, s.ctx->B32, pl->d_sum, tile0, (ScenDesc<float> *)slot);
@@ -129,19 +139,48 @@ static int rebuild_table(swehr_pool *pl)
         cells += s.cells;
         k++;
     }
-    BatchHdr<double> h;   /* same layout for both forms: a pointer, two ints, a count */
+    /* tile -> scenario map (grown on demand; nothing is in flight here) */
+    if (tile0 > pl->map_cap) {
+        PCK(cudaStreamSynchronize(pl->stream));
+        const int64_t cap = std::max(tile0, 2 * pl->map_cap);
+        if (pl->d_map) cudaFree(pl->d_map);
+        if (pl->h_map) cudaFreeHost(pl->h_map);
+        pl->d_map = nullptr;
+        pl->h_map = nullptr;
+        pl->map_cap = 0;
+        PCK(cudaMalloc((void **)&pl->d_map, (size_t)cap * sizeof(int32_t)));
+        PCK(cudaMallocHost((void **)&pl->h_map, (size_t)cap * sizeof(int32_t)));
+        pl->map_cap = cap;
+    }
+    {
+        int64_t at = 0;
+        int sid = 0;
+        for (auto &s : pl->scen) {
+            if (!s.running) continue;
+            for (int64_t t = 0; t < s.ntiles; t++) pl->h_map[at + t] = sid;
+            at += s.ntiles;
+            sid++;
+        }
+    }
+    BatchHdr<double> h;   /* same layout for both forms: pointers and counts */
     static_assert(sizeof(BatchHdr<double>) == sizeof(BatchHdr<float>), "header layout");
+    memset(&h, 0, sizeof h);
     h.tab = (const ScenDesc<double> *)pl->d_tab;
     h.nscen = k;
     h.pad = 0;
     h.total_tiles = tile0;
+    h.tile_scen = pl->d_map;
     memcpy(pl->h_hdr, &h, sizeof h);
     if (k > 0) PCK(cudaMemcpyAsync(pl->d_tab, pl->h_tab, (size_t)k * pl->desc_bytes, cudaMemcpyHostToDevice, pl->stream));
+    if (tile0 > 0)
+        PCK(cudaMemcpyAsync(pl->d_map, pl->h_map, (size_t)tile0 * sizeof(int32_t), cudaMemcpyHostToDevice, pl->stream));
     PCK(cudaMemcpyAsync(pl->d_hdr, pl->h_hdr, sizeof h, cudaMemcpyHostToDevice, pl->stream));
     pl->nrun = k;
     pl->total_tiles = tile0;
     pl->running_cells = cells;
+    pl->max_s = max_s;
     pl->dirty = false;
+    apply_shape(pl);
     return SWEHR_OK;
 }
 
@@ -151,7 +190,7 @@ static void launch_pool_step(swehr_pool *pl, cudaEvent_t e0, cudaEvent_t e1, cud
     if (e0) cudaEventRecord(e0, pl->stream);
     cudaLaunchKernel(pl->cfg.fn_wave, dim3(pl->grid_wave), dim3(pl->cfg.threads), args, pl->cfg.smem_wave, pl->stream);
     if (e1) cudaEventRecord(e1, pl->stream);
-    cudaLaunchKernel(pl->cfg.fn_update, dim3(pl->grid_update), dim3(pl->cfg.threads), args, pl->cfg.smem_update,
+    cudaLaunchKernel(pl->cfg.fn_update, dim3(pl->grid_update), dim3(pl->cfg.threads), args, pl->smem_update,
                      pl->stream);
     if (e2) cudaEventRecord(e2, pl->stream);
 }
@@ -177,6 +216,24 @@ static void set_grids(swehr_pool *pl, int kw, int ku)
     }
     pl->grid_wave = pl->num_sms * kw;
     pl->grid_update = pl->num_sms * ku;
+}
+
+/* shared memory and grids for the scenarios running now: the update
+ * kernel's staging is sized by the largest class count present, so a pool
+ * that admits up to 16 classes still runs 7-class batches at the 7-class
+ * occupancy */
+static void apply_shape(swehr_pool *pl)
+{
+    const size_t sm = pl->cfg.smem_update_s[pl->max_s];
+    if (sm != pl->smem_update) {
+        if (pl->graph) cudaGraphExecDestroy(pl->graph);
+        pl->graph = nullptr;
+        pl->smem_update = sm;
+    }
+    const int occ_u = pl->cfg.occ_update_s[pl->max_s];
+    const int ku = pl->ku_sel ? std::min(pl->ku_sel, occ_u) : occ_u;
+    const int kw = pl->kw_sel ? pl->kw_sel : pl->cfg.occ_wave;
+    set_grids(pl, kw, ku);
 }
 
 /* copy the summaries back (after the stream's work) and fold them in */
@@ -259,7 +316,6 @@ int swehr_pool_create(int precision, int max_classes, int budget, size_t hbm_lim
             return rc;
         }
     }
-    set_grids(pl, pl->cfg.occ_wave, pl->cfg.occ_update);
     PCKF(cudaStreamCreateWithFlags(&pl->stream, cudaStreamNonBlocking));
     PCKF(cudaEventCreate(&pl->ev0));
     PCKF(cudaEventCreate(&pl->ev1));
@@ -389,22 +445,31 @@ int swehr_pool_tune(swehr_pool *pl, int64_t steps_per_trial, swehr_pool_stats *s
     if (steps_per_trial < 1 || steps_per_trial > 4096) return swehr_err(SWEHR_INVALID, "steps_per_trial must be 1..4096");
     swehr_pool_stats local;
     memset(&local, 0, sizeof local);
-    const int trials = std::max(pl->cfg.occ_wave, pl->cfg.occ_update);
+    if (pl->dirty) {
+        int rc = rebuild_table(pl);
+        if (rc) return rc;
+    }
+    const int occ_u = pl->cfg.occ_update_s[pl->max_s];
+    const int trials = std::max(pl->cfg.occ_wave, occ_u);
     const size_t need = (size_t)3 * steps_per_trial;
     while (pl->ev_ring.size() < need) {
         cudaEvent_t e;
         PCK(cudaEventCreate(&e));
         pl->ev_ring.push_back(e);
     }
-    double best_w = INFINITY, best_u = INFINITY;
-    int kw_best = pl->cfg.occ_wave, ku_best = pl->cfg.occ_update;
-    for (int k = 1; k <= trials; k++) {
+    /* every candidate is timed in each of kRounds round-robin passes and
+     * keeps its best time per tile, so the state drifting between trials
+     * and one-off noise do not decide */
+    const int kRounds = 3;
+    std::vector<double> bw((size_t)trials + 1, INFINITY), bu((size_t)trials + 1, INFINITY);
+    for (int trial = 0; trial < kRounds * trials; trial++) {
+        const int k = 1 + trial % trials;
         if (pl->dirty) {
             int rc = rebuild_table(pl);
             if (rc) return rc;
         }
         if (pl->nrun == 0) break;
-        const int kw = std::min(k, pl->cfg.occ_wave), ku = std::min(k, pl->cfg.occ_update);
+        const int kw = std::min(k, pl->cfg.occ_wave), ku = std::min(k, occ_u);
         set_grids(pl, kw, ku);
         const int64_t tiles = pl->total_tiles;
         for (int64_t s = 0; s < steps_per_trial; s++)
@@ -424,9 +489,16 @@ int swehr_pool_tune(swehr_pool *pl, int64_t steps_per_trial, swehr_pool_stats *s
         local.device_ms += w + u;
         w /= (double)tiles;
         u /= (double)tiles;
-        if (kw == k && w < best_w) { best_w = w; kw_best = kw; }
-        if (ku == k && u < best_u) { best_u = u; ku_best = ku; }
+        if (kw == k) bw[k] = std::min(bw[k], w);
+        if (ku == k) bu[k] = std::min(bu[k], u);
     }
+    int kw_best = pl->cfg.occ_wave, ku_best = occ_u;
+    for (int k = 1; k <= trials; k++) {
+        if (bw[k] < bw[kw_best]) kw_best = k;
+        if (bu[k] < bu[ku_best]) ku_best = k;
+    }
+    pl->kw_sel = kw_best;
+    pl->ku_sel = ku_best;
     set_grids(pl, kw_best, ku_best);
     pl->tuned = 1;
     fill_stats(pl, &local);

@@ -193,6 +193,9 @@ __device__ __forceinline__ TileCoord tile_coord(const DevParams &P, int64_t tile
 #define ZP_ROWS 12
 #define ZC_ROWS 10
 
+static_assert((size_t)(TILE_THREADS / 32) * B_NTERMS * sizeof(double) <= 4 * N_H * sizeof(float),
+              "budget reduction fits in the face-state arrays it reuses");
+
 struct StagedLayout {
     /* byte offsets from the start of dynamic shared memory */
     size_t halo, cell_r, cell_d, zp, zc, u, v, g, c, sed, fx, fy, up, red, total;
@@ -218,7 +221,9 @@ struct StagedLayout {
         L.fx = take(what ? (size_t)3 * N_FX * rs : 0);
         L.fy = take(what ? (size_t)3 * N_FY * rs : 0);
         L.up = take(what ? (size_t)(N_FX + N_FY) : 0);
-        L.red = take(what ? (size_t)(TILE_THREADS / 32) * B_NTERMS * sizeof(double) : 0);
+        /* the budget reduction runs after a tile's cells are done, when the
+         * face states u, v, g, c are dead: it reuses their space */
+        L.red = L.u;
         L.total = o;
         return L;
     }
@@ -1112,15 +1117,21 @@ __global__ void __launch_bounds__(TILE_THREADS, PP::kMinBlocks) k_update_tile(co
  * arithmetic, so every scenario's result is identical alone or in a batch.
  * Budget sums of a batched step are block partials added with atomics
  * (order-dependent rounding of the budget terms only). */
+/* Copy scenario sid's descriptor into the block's shared copy unless it is
+ * already there (the whole block calls it; sid is uniform).  Parameters then
+ * come from a shared object no other store can alias, instead of global
+ * memory the compiler would have to re-read after every store. */
 template <class RS>
-__device__ __forceinline__ int scen_of(const ScenDesc<RS> *tab, int nscen, int64_t g)
+__device__ __forceinline__ void load_desc(const ScenDesc<RS> *tab, int sid, ScenDesc<RS> &sd, int &cur)
 {
-    int lo = 0, hi = nscen - 1;
-    while (lo < hi) {
-        const int mid = (lo + hi + 1) >> 1;
-        if (tab[mid].tile0 <= g) lo = mid; else hi = mid - 1;
-    }
-    return lo;
+    if (sid == cur) return;
+    static_assert(sizeof(ScenDesc<RS>) % 8 == 0, "descriptor copied in 8-byte words");
+    const unsigned long long *src = reinterpret_cast<const unsigned long long *>(tab + sid);
+    unsigned long long *dst = reinterpret_cast<unsigned long long *>(&sd);
+    __syncthreads();                                             /* previous tile is done with sd */
+    for (int w = threadIdx.x; w < (int)(sizeof(ScenDesc<RS>) / 8); w += blockDim.x) dst[w] = src[w];
+    __syncthreads();
+    cur = sid;
 }
 
 template <class PP, class RS>
@@ -1129,22 +1140,33 @@ __global__ void __launch_bounds__(TILE_THREADS) k_wave_batch(const BatchHdr<RS> 
     typedef typename PP::R R;
     extern __shared__ __align__(16) unsigned char smb[];
     __shared__ double red8[TILE_THREADS / 32];
+    __shared__ __align__(16) ScenDesc<RS> sd;
     const StagedLayout L = StagedLayout::make(0, sizeof(R), 0);
     const ScenDesc<RS> *tab = hdr->tab;
-    const int nscen = hdr->nscen;
+    const int32_t *map = hdr->tile_scen;
     const int64_t total = hdr->total_tiles;
+    int cur = -1;
+    int sid_next = blockIdx.x < total ? map[blockIdx.x] : 0;
     for (int64_t g = blockIdx.x; g < total; g += gridDim.x) {
-        const ScenDesc<RS> &D = tab[scen_of(tab, nscen, g)];
+        const int sid = sid_next;                                /* uniform across the block */
+        if (g + gridDim.x < total) sid_next = map[g + gridDim.x];
+        load_desc(tab, sid, sd, cur);
+        const ScenDesc<RS> &D = sd;
         Ctl *ctl = D.ctl;
-        if (!ctl->active) continue;                              /* uniform across the block */
+        if (!ctl->active) continue;
         const int64_t n = ctl->step;
+        const double t = ctl->t;
         const R s = wave_tile<PP, RS>(D.P, D.B.set[n & 1], D.B.z[(n + 2) % 3], tile_coord(D.P, g - D.tile0), smb, L,
-                                      ctl->t);
+                                      t);
         const double m = block_max((double)s, red8);
         if (threadIdx.x == 0) {
             atomicMax(&ctl->smax_bits, (unsigned long long)__double_as_longlong(m));
             __threadfence();
-            if (atomicAdd(&ctl->wave_ticket, 1u) == (unsigned)(D.ntiles - 1)) wave_finalize(D.P, ctl);
+            if (atomicAdd(&ctl->wave_ticket, 1u) == (unsigned)(D.ntiles - 1)) {
+                wave_finalize(D.P, ctl);
+                /* the step's uniform rain rate, read by every update tile */
+                ctl->rain_now = D.P.storm ? 0.0 : rain_at(D.P, D.rain, t);
+            }
         }
         __syncthreads();
     }
@@ -1156,34 +1178,42 @@ __global__ void __launch_bounds__(TILE_THREADS, PP::kMinBlocks) k_update_batch(c
     typedef typename PP::R R;
     extern __shared__ __align__(16) unsigned char smb[];
     __shared__ bool last;
+    __shared__ __align__(16) ScenDesc<RS> sd;
     const ScenDesc<RS> *tab = hdr->tab;
-    const int nscen = hdr->nscen;
+    const int32_t *map = hdr->tile_scen;
     const int64_t total = hdr->total_tiles;
+    int cur = -1;
+    int sid_next = blockIdx.x < total ? map[blockIdx.x] : 0;
     for (int64_t g = blockIdx.x; g < total; g += gridDim.x) {
-        const ScenDesc<RS> &D = tab[scen_of(tab, nscen, g)];
+        const int sid = sid_next;                                /* uniform across the block */
+        if (g + gridDim.x < total) sid_next = map[g + gridDim.x];
+        load_desc(tab, sid, sd, cur);
+        const ScenDesc<RS> &D = sd;
         Ctl *ctl = D.ctl;
-        if (!ctl->pending) continue;                             /* uniform across the block */
+        if (!ctl->pending) continue;
         const StagedLayout L = StagedLayout::make(D.P.S, sizeof(R), 1);
         const int64_t n = ctl->step;
-        const double t = ctl->t, dt = ctl->dt;
-        const double Rr = D.P.storm ? 0.0 : rain_at(D.P, D.rain, t);
+        const double t = ctl->t, dt = ctl->dt, Rr = ctl->rain_now;
         Acc2<MAXS, BUDGET> acc;
         acc_zero(acc);
         update_tile<PP, RS, MAXS, BUDGET>(D.P, D.B, n, t, dt, Rr, tile_coord(D.P, g - D.tile0), smb, L, acc);
         double *red = reinterpret_cast<double *>(smb + L.red);
         const bool bud = BUDGET && D.P.budget;
         if (bud) budget_block_sum(acc, red);
-        __threadfence();
         __syncthreads();
+        /* release this tile's writes, count it; the scenario's last tile
+         * acquires everyone's writes before finalizing (one thread fences
+         * on either side of the barrier) */
         if (threadIdx.x == 0) {
             if (bud)
                 for (int m = 0; m < B_NTERMS; m++) atomicAdd(&ctl->budget_step[m], red[m]);
             __threadfence();
-            last = (atomicAdd(&ctl->update_ticket, 1u) == (unsigned)(D.ntiles - 1));
+            const bool l = atomicAdd(&ctl->update_ticket, 1u) == (unsigned)(D.ntiles - 1);
+            if (l) __threadfence();
+            last = l;
         }
         __syncthreads();
         if (last) {
-            __threadfence();
             if (bud && threadIdx.x < B_NTERMS) {
                 const double v = atomicAdd(&ctl->budget_step[threadIdx.x], 0.0);
                 ctl->budget_step[threadIdx.x] = 0.0;

@@ -23,7 +23,8 @@ import pytest
 
 from harness import compare
 from swehr_b200 import workloads as W
-from swehr_b200.params import FP64, MIXED, REFERENCE_DEFAULTS
+from swehr_b200.accuracy import quantized_case
+from swehr_b200.params import FP64, MIXED
 
 pytestmark = pytest.mark.gpu
 
@@ -39,27 +40,8 @@ def _run(case, precision, steps=-1, budget=False):
         return pr, s.fields(), (s.budget() if budget else None)
 
 
-def _f32(x):
-    return float(np.float32(x))
-
-
-# parameters the mixed form keeps in FP64 (time stepping, Green-Ampt, storm track)
-KEEP64 = {"dx", "tend", "rint", "stageint", "thetas", "theta0", "hf", "ks", "vinf0", "cstable", "maxstep",
-          "storm_peak", "storm_radius", "storm_x0", "storm_y0", "storm_vx", "storm_vy"}
-
-
 def quantized(case):
-    """The case with every real input the mixed form holds in FP32 rounded to
-    FP32 (z, Green-Ampt and time stepping stay FP64, as in the mixed form)."""
-    p = dict(REFERENCE_DEFAULTS)
-    p.update(case.params)
-    for k, v in list(p.items()):
-        if isinstance(v, float) and k not in KEEP64:
-            p[k] = _f32(v)
-    ks = None if case.ks is None else case.ks.astype(np.float32).astype(np.float64)
-    return W.Case(case.name + "_q32", p, case.topo, case.rain.astype(np.float32).astype(np.float64),
-                  case.ds.astype(np.float32).astype(np.float64), case.pfrac.astype(np.float32).astype(np.float64),
-                  ks=ks, max_steps=case.max_steps)
+    return quantized_case(case)
 
 
 def _err(a, b):
