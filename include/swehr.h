@@ -119,7 +119,7 @@ typedef struct swehr_progress {
     double  t;              /* simulated time after the last completed step */
     double  dt;             /* last time step */
     double  courant;        /* last Courant number */
-    double  rain;           /* last uniform rain rate */
+    double  rain;           /* uniform rain rate of the last step (0 with a moving storm) */
     int64_t steps;          /* steps completed since swehr_create */
     int64_t steps_this_call;
     double  device_ms;      /* device time of this call, CUDA events on the context stream */
@@ -127,6 +127,7 @@ typedef struct swehr_progress {
     int64_t kernel_launches;/* kernels this call launched */
     int32_t status;
     int32_t done;           /* 1 when t >= tend */
+    double  t_step;         /* start time of the last completed step (the time a CFL error is reported at) */
 } swehr_progress;
 
 /* Water / sediment budget (an addition; the reference keeps none).  All sums

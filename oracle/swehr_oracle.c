@@ -80,6 +80,7 @@ typedef struct orc_ctx {
     double *srcf;                 /* per-cell sources: SXf SYf GAMMAX GAMMAY DFMASK BETAX BETAY FAIL GZ */
     double *E, *VF;               /* [(4*k + e)*N + c], [k*N + c] */
     double t, dt, courant, R;
+    double t_prev;                /* start time of the last completed step */
     int64_t steps;
     int status;
     /* stage series */
@@ -517,6 +518,7 @@ static int orc_step(orc_ctx *c)
     c->dt = dt;
     c->courant = courant;
     c->R = R;
+    c->t_prev = t;
     c->t = cfl ? 2 * p->tend : t;
     c->t += dt;
     c->steps++;
@@ -634,6 +636,7 @@ int orc_advance(orc_ctx *c, double t_stop, int64_t max_steps, swehr_progress *pr
         pr->t = c->t; pr->dt = c->dt; pr->courant = c->courant; pr->rain = c->R;
         pr->steps = c->steps; pr->steps_this_call = n; pr->status = st;
         pr->done = c->t >= c->p.tend;
+        pr->t_step = c->t_prev;
     }
     return st;
 }

@@ -62,7 +62,23 @@ def build(verbose: bool = False, ptxas_v: bool = False) -> str:
     if verbose:
         print(" ".join(cmd))
     subprocess.check_call(cmd)
+    build_driver(verbose)
     return OUT
+
+
+DRIVER = os.path.join(HERE, "swehr_gpu")
+
+
+def build_driver(verbose: bool = False) -> str:
+    """The command-line host (plain C, linked against libswehr.so beside it)."""
+    src = os.path.join(CSRC, "swehr_gpu.c")
+    cmd = ["gcc", "-O2", "-std=c11", "-D_POSIX_C_SOURCE=200809L", "-Wall", "-Wextra", "-Werror",
+           "-I", os.path.join(HERE, "..", "include"), src, "-o", DRIVER, "-L", HERE, "-lswehr",
+           "-Wl,-rpath,$ORIGIN", "-lm"]
+    if verbose:
+        print(" ".join(cmd))
+    subprocess.check_call(cmd)
+    return DRIVER
 
 
 def main():

@@ -440,6 +440,7 @@ extern "C" int swehr_advance(swehr_ctx *c, double t_stop, int64_t max_steps, swe
         if (pr) {
             memset(pr, 0, sizeof *pr);
             pr->t = h->t; pr->steps = h->step; pr->status = SWEHR_CFL_ERROR; pr->done = 1;
+            pr->dt = h->dt; pr->courant = h->courant; pr->rain = h->rain_now; pr->t_step = h->t_prev;
         }
         return SWEHR_CFL_ERROR;
     }
@@ -504,7 +505,8 @@ extern "C" int swehr_advance(swehr_ctx *c, double t_stop, int64_t max_steps, swe
     if (pr) {
         memset(pr, 0, sizeof *pr);
         pr->t = h->t; pr->dt = h->dt; pr->courant = h->courant;
-        pr->rain = 0;
+        pr->rain = h->rain_now;
+        pr->t_step = h->t_prev;
         pr->steps = h->step;
         pr->steps_this_call = h->step - step0;
         pr->device_ms = dev_ms;

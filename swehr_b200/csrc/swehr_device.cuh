@@ -87,7 +87,8 @@ struct Ctl {
     int64_t launches;
     double budget_hi[64], budget_lo[64];   /* running compensated budget sums */
     double budget_step[64];                 /* this step's partials in batched mode */
-    double rain_now;                        /* batched mode: uniform rain rate of the pending step */
+    double rain_now;                        /* uniform rain rate of the current / last step */
+    double t_prev;                          /* start time of the last completed step */
     double sed0[16];
 };
 

@@ -1046,6 +1046,7 @@ __device__ __forceinline__ void update_finalize(const DevParams &P, const SetV<R
     if (stage_due) stage_sample_tile<PP, RS>(P, dst, ctl, tnew, stage, saveflow, reinterpret_cast<double *>(smb));
     __syncthreads();
     if (threadIdx.x == 0) {
+        ctl->t_prev = t;
         ctl->t = tnew;
         ctl->step = n + 1;
         ctl->pending = 0;
@@ -1104,6 +1105,7 @@ __global__ void __launch_bounds__(TILE_THREADS, PP::kMinBlocks) k_update_tile(co
             dd_add(hi, lo, ((volatile double *)partials)[(int64_t)b * B_NTERMS + threadIdx.x]);
         budget_fold(ctl, threadIdx.x, hi, lo);
     }
+    if (threadIdx.x == 0) ctl->rain_now = Rr;
     update_finalize<PP, RS>(P, B.set[(n + 1) & 1], ctl, stage, saveflow, smb);
 }
 

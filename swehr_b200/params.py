@@ -62,7 +62,7 @@ class SwehrProgress(C.Structure):
         ("t", C.c_double), ("dt", C.c_double), ("courant", C.c_double), ("rain", C.c_double),
         ("steps", C.c_int64), ("steps_this_call", C.c_int64),
         ("device_ms", C.c_double), ("kernel_ms", C.c_double), ("kernel_launches", C.c_int64),
-        ("status", C.c_int32), ("done", C.c_int32),
+        ("status", C.c_int32), ("done", C.c_int32), ("t_step", C.c_double),
     ]
 
 

@@ -12,6 +12,11 @@ oracle/build_ref.py, on:
                     on and off, per-cell Ks, to the end of their event
   hillslope.npz     the 200x50 hillslope, full 1200 s run, and the state at
                     600 s (mid-event, wet)
+  shipped_files.npz the reference's own output files for the shipped
+                    example run as shipped (movies on): the ten result
+                    grids, stage.txt, saveflow.txt, every 30th frame of the
+                    five movie files, the console's per-frame lines and its
+                    header (the host driver's parity target)
 
 Each file holds the Case (params as JSON, topo, rain, ds, pfrac, ks) and the
 reference's %.17g dump of every state field.
@@ -70,14 +75,65 @@ def shipped_case(reference):
     return c
 
 
+RESULT_FILES = ("topoout", "depth", "uh", "vh", "ch", "m", "c", "vel", "maxvel", "maxdepth")
+MOVIE_FILES = ("topomovie", "depthmovie", "velocitymovie", "cmovie", "Mmovie")
+FRAME_STRIDE = 30
+
+
+def read_table(path):
+    with open(path) as f:
+        return np.array([[float(v) for v in line.split()] for line in f if line.strip()])
+
+
+def shipped_files(reference):
+    """Run the reference binary on the shipped input files exactly as shipped
+    and parse everything it writes."""
+    import shutil
+    import subprocess
+    import tempfile
+    wd = tempfile.mkdtemp(prefix="swehr_files_")
+    for fn in ("input.txt", "rain.txt", "particlesizein.txt", "particlepercentin.txt", "topoin.txt"):
+        shutil.copy(os.path.join(reference, fn), wd)
+    r = subprocess.run([harness.ref_binary(False)], cwd=wd, capture_output=True, text=True, timeout=3600)
+    if r.returncode != 0:
+        raise RuntimeError(r.stderr[-2000:])
+    lines = r.stdout.splitlines()
+    frames = [ln for ln in lines if ln.count("\t") == 3 and not ln.startswith(("Point", "SWEHR"))]
+    header = [ln for ln in lines if ln.split(":")[0] in ("Grid Size (Spacing)", "Number of conserved variables",
+                                                          "Number of particle size classes", "a0", "ad0", "F",
+                                                          "J", "h0", "mtstar0", "b", "Basin Outlet Pixel",
+                                                          "Basin Outlet Elevation (m)")
+              or ln.startswith("Point ") or ln.startswith("H-R Parameters")]
+    arrs = {"header": np.array("\n".join(header)),
+            "frame_lines": np.array([[float(v) for v in ln.split()] for ln in frames])}
+    ny = int(read_table(os.path.join(wd, "depth.txt")).shape[0])
+    for n in RESULT_FILES:
+        arrs[n] = read_table(os.path.join(wd, n + ".txt"))
+    arrs["stage"] = read_table(os.path.join(wd, "stage.txt"))
+    arrs["saveflow"] = read_table(os.path.join(wd, "saveflow.txt"))
+    for n in MOVIE_FILES:
+        m = read_table(os.path.join(wd, n + ".txt"))
+        arrs[n + "_frames"] = np.array(m.shape[0] // ny)
+        arrs[n] = m.reshape(-1, ny, m.shape[1])[::FRAME_STRIDE]
+    arrs["frame_stride"] = np.array(FRAME_STRIDE)
+    shutil.rmtree(wd, ignore_errors=True)
+    path = os.path.join(HERE, "shipped_files.npz")
+    np.savez_compressed(path, **arrs)
+    print("wrote", path, os.path.getsize(path), "bytes")
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--reference", default="/root/reference")
+    ap.add_argument("--only", default=None, help="shipped_files: only regenerate that fixture")
     a = ap.parse_args()
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import build_ref
     if not build_ref.build(a.reference):
         raise SystemExit("reference not available")
+    if a.only == "shipped_files":
+        shipped_files(a.reference)
+        return
     c = shipped_case(a.reference)
     d1, _ = harness.run_reference(c, max_steps=2000)
     d2, _ = harness.run_reference(c, max_steps=20000)
@@ -95,6 +151,7 @@ def main():
     dmid, _ = harness.run_reference(c600)
     dend, _ = harness.run_reference(c)
     save(os.path.join(HERE, "hillslope.npz"), c, {"t600": dmid, "end": dend})
+    shipped_files(a.reference)
 
 
 if __name__ == "__main__":
