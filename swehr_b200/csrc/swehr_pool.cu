@@ -56,7 +56,12 @@ struct swehr_pool {
     int max_s = 1;                       /* largest class count running */
     size_t smem_update = 0;              /* update kernel's dynamic shared memory now */
     cudaStream_t stream = nullptr;
-    cudaGraphExec_t graph = nullptr;
+    struct GraphEntry {
+        size_t smem;
+        int gw, gu;
+        cudaGraphExec_t exec;
+    };
+    std::vector<GraphEntry> graphs;      /* one per launch shape seen (class count x grids) */
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     std::vector<cudaEvent_t> ev_ring;   /* tuner: 3 events per step */
     char *d_hdr = nullptr, *h_hdr = nullptr;
@@ -87,7 +92,7 @@ static void pool_free(swehr_pool *pl)
     if (pl->stream) cudaStreamSynchronize(pl->stream);
     for (auto &s : pl->scen) swehr_ctx_destroy(s.ctx);
     pl->scen.clear();
-    if (pl->graph) cudaGraphExecDestroy(pl->graph);
+    for (auto &g : pl->graphs) cudaGraphExecDestroy(g.exec);
     if (pl->ev0) cudaEventDestroy(pl->ev0);
     if (pl->ev1) cudaEventDestroy(pl->ev1);
     for (cudaEvent_t e : pl->ev_ring) cudaEventDestroy(e);
@@ -195,25 +200,32 @@ static void launch_pool_step(swehr_pool *pl, cudaEvent_t e0, cudaEvent_t e1, cud
     if (e2) cudaEventRecord(e2, pl->stream);
 }
 
-static int build_pool_graph(swehr_pool *pl)
+/* The graph of GRAPH_STEPS pool steps for the current launch shape, built
+ * on first use and kept: serving mixes change the largest class count (and
+ * with it the staging size and grid) as scenarios come and go, and a shape
+ * seen once is usually seen again. */
+static int pool_graph(swehr_pool *pl, cudaGraphExec_t *out)
 {
-    if (pl->graph) return SWEHR_OK;
+    for (auto &g : pl->graphs)
+        if (g.smem == pl->smem_update && g.gw == pl->grid_wave && g.gu == pl->grid_update) {
+            *out = g.exec;
+            return SWEHR_OK;
+        }
     cudaGraph_t g;
     PCK(cudaStreamBeginCapture(pl->stream, cudaStreamCaptureModeThreadLocal));
     for (int s = 0; s < GRAPH_STEPS; s++) launch_pool_step(pl, nullptr, nullptr, nullptr);
     PCK(cudaStreamEndCapture(pl->stream, &g));
-    cudaError_t e = cudaGraphInstantiate(&pl->graph, g, 0);
+    cudaGraphExec_t ex = nullptr;
+    cudaError_t e = cudaGraphInstantiate(&ex, g, 0);
     cudaGraphDestroy(g);
     if (e != cudaSuccess) return swehr_err(SWEHR_CUDA_ERROR, std::string("cudaGraphInstantiate: ") + cudaGetErrorString(e));
+    pl->graphs.push_back({pl->smem_update, pl->grid_wave, pl->grid_update, ex});
+    *out = ex;
     return SWEHR_OK;
 }
 
 static void set_grids(swehr_pool *pl, int kw, int ku)
 {
-    if (pl->grid_wave != pl->num_sms * kw || pl->grid_update != pl->num_sms * ku) {
-        if (pl->graph) cudaGraphExecDestroy(pl->graph);
-        pl->graph = nullptr;
-    }
     pl->grid_wave = pl->num_sms * kw;
     pl->grid_update = pl->num_sms * ku;
 }
@@ -224,12 +236,7 @@ static void set_grids(swehr_pool *pl, int kw, int ku)
  * occupancy */
 static void apply_shape(swehr_pool *pl)
 {
-    const size_t sm = pl->cfg.smem_update_s[pl->max_s];
-    if (sm != pl->smem_update) {
-        if (pl->graph) cudaGraphExecDestroy(pl->graph);
-        pl->graph = nullptr;
-        pl->smem_update = sm;
-    }
+    pl->smem_update = pl->cfg.smem_update_s[pl->max_s];
     const int occ_u = pl->cfg.occ_update_s[pl->max_s];
     const int ku = pl->ku_sel ? std::min(pl->ku_sel, occ_u) : occ_u;
     const int kw = pl->kw_sel ? pl->kw_sel : pl->cfg.occ_wave;
@@ -407,12 +414,16 @@ int swehr_pool_run(swehr_pool *pl, int64_t steps, swehr_pool_stats *st)
     }
     float ms = 0;
     if (pl->nrun > 0 && steps != 0) {
-        int rc = build_pool_graph(pl);
-        if (rc) return rc;
+        cudaGraphExec_t graph = nullptr;
+        if (steps < 0 || steps >= GRAPH_STEPS) {
+            int rc = pool_graph(pl, &graph);
+            if (rc) return rc;
+        }
+        int rc = SWEHR_OK;
         PCK(cudaEventRecord(pl->ev0, pl->stream));
         if (steps > 0) {
             const int64_t full = steps / GRAPH_STEPS, rem = steps % GRAPH_STEPS;
-            for (int64_t g = 0; g < full; g++) PCK(cudaGraphLaunch(pl->graph, pl->stream));
+            for (int64_t g = 0; g < full; g++) PCK(cudaGraphLaunch(graph, pl->stream));
             for (int64_t s = 0; s < rem; s++) launch_pool_step(pl, nullptr, nullptr, nullptr);
             PCK(cudaGetLastError());
             local.pool_steps = steps;
@@ -421,7 +432,7 @@ int swehr_pool_run(swehr_pool *pl, int64_t steps, swehr_pool_stats *st)
             if (rc) return rc;
         } else {
             for (;;) {
-                for (int g = 0; g < 4; g++) PCK(cudaGraphLaunch(pl->graph, pl->stream));
+                for (int g = 0; g < 4; g++) PCK(cudaGraphLaunch(graph, pl->stream));
                 local.pool_steps += 4 * GRAPH_STEPS;
                 PCK(cudaEventRecord(pl->ev1, pl->stream));
                 rc = collect(pl, &local);

@@ -135,6 +135,7 @@ class Report:
     peak_hbm_bytes: int
     hbm_limit: int
     results: List[Result]
+    host_s: Dict[str, float] = field(default_factory=dict)   # wall time per loop phase
 
     @property
     def cell_steps_per_s(self) -> float:
@@ -147,7 +148,7 @@ class Report:
                 "pool_steps": self.pool_steps, "cell_steps_per_s": self.cell_steps_per_s,
                 "p50_s": self.p50_s, "p99_s": self.p99_s, "mean_s": self.mean_s,
                 "max_resident": self.max_resident, "peak_hbm_bytes": self.peak_hbm_bytes,
-                "hbm_limit": self.hbm_limit}
+                "hbm_limit": self.hbm_limit, "host_s": self.host_s}
 
 
 def percentile(xs: Sequence[float], q: float) -> Optional[float]:
@@ -202,6 +203,8 @@ class Server:
         device_ms = 0.0
         max_res = peak_hbm = 0
         hbm_limit = 0
+        host = {"submit_s": 0.0, "run_s": 0.0, "poll_s": 0.0, "read_s": 0.0, "release_s": 0.0}
+        clk = self.clock
         while nxt < len(reqs) or queue or live:
             now = self.clock() - t0
             if time_limit is not None and now >= time_limit:
@@ -213,8 +216,10 @@ class Server:
             while queue:
                 r = queue[0]
                 case = r.case if r.case is not None else make_case(r)
+                ts = clk()
                 try:
                     sc = pool.submit(case)
+                    host["submit_s"] += clk() - ts
                 except Exception as e:  # noqa: BLE001 -- a request the pool can never hold
                     if getattr(e, "status", None) != INVALID:
                         raise
@@ -230,22 +235,32 @@ class Server:
                     self.sleep(max(0.0, min(reqs[nxt].arrival - (self.clock() - t0), 0.05)))
                     continue
                 break
+            ts = clk()
             st = pool.run(self.chunk_steps)
+            host["run_s"] += clk() - ts
             cell_steps += int(st.cell_steps)
             pool_steps += int(st.pool_steps)
             device_ms += float(st.device_ms)
             max_res = max(max_res, int(st.resident))
             peak_hbm = max(peak_hbm, int(st.hbm_used))
             hbm_limit = int(st.hbm_limit)
+            ts = clk()
+            done = []
             for rid in list(live):
+                pr = live[rid][1].progress()
+                if pr.done:
+                    done.append((rid, pr))
+            host["poll_s"] += clk() - ts
+            for rid, pr in done:
                 r, sc, adm = live[rid]
-                pr = sc.progress()
-                if not pr.done:
-                    continue
+                ts = clk()
                 out = sc.fields(self.result_fields)
-                fin = self.clock() - t0
+                fin = clk() - t0
+                host["read_s"] += clk() - ts
                 res = Result(rid, r.arrival, adm, fin, int(pr.steps), int(pr.status), r.cells, out)
+                ts = clk()
                 pool.release(sc)
+                host["release_s"] += clk() - ts
                 del live[rid]
                 results.append(res)
                 if on_result is not None:
@@ -257,4 +272,4 @@ class Server:
                       wall_s=wall, device_ms=device_ms, cell_steps=cell_steps, pool_steps=pool_steps,
                       p50_s=percentile(lat, 50), p99_s=percentile(lat, 99),
                       mean_s=(sum(lat) / len(lat)) if lat else None, max_resident=max_res,
-                      peak_hbm_bytes=peak_hbm, hbm_limit=hbm_limit, results=results)
+                      peak_hbm_bytes=peak_hbm, hbm_limit=hbm_limit, results=results, host_s=host)
