@@ -52,6 +52,21 @@ def algo_bytes_mixed(S: int) -> int:
     return 2 * (4 * (5 + S) + 8 * (2 + S)) + 4
 
 
+def profiled_traffic(summary: str):
+    """DRAM bytes per cell-step of a kernel, from its committed ncu summary
+    (dram__bytes_read.sum + dram__bytes_write.sum of one captured launch on
+    a 1024^2 case, divided by its cells; per-cell traffic is size
+    independent once the state is far larger than L2)."""
+    path = os.path.join(ROOT, "profiles", summary)
+    try:
+        for line in open(path):
+            if line.startswith("traffic_bytes_per_cell_step:"):
+                return float(line.split(":")[1])
+    except OSError:
+        pass
+    return None
+
+
 def hbm_peak():
     try:
         with open(PEAKS_PATH) as f:
@@ -354,11 +369,15 @@ def main():
         vm = world * cells * prm.steps_this_call / (em / 1e3)
         um = prm.kernel_ms / max(prm.steps_this_call, 1)
         Bm = algo_bytes_mixed(S)
+        tm = profiled_traffic("k_update_tile_f32_fractal1024.md")
         mixed = {"value": vm, "unit": "cell-steps/s", "ms_per_step": em / max(prm.steps_this_call, 1),
                  "steps": int(prm.steps_this_call), "gpu_launches": int(prm.kernel_launches),
                  "over_fp64": vm / value,
                  "roofline": {"bound": "hbm", "achieved": Bm * cells / (um / 1e3) / 1e9 if um > 0 else None,
-                              "unit": "GB/s", "algo_bytes_per_cell_step": Bm, "update_ms_avg": um},
+                              "peak": hbm_peak()[0], "unit": "GB/s",
+                              "frac": (Bm * cells / (um / 1e3) / 1e9 / hbm_peak()[0]) if um > 0 else None,
+                              "traffic": tm * cells if tm else None,
+                              "algo_bytes_per_cell_step": Bm, "update_ms_avg": um},
                  "dtype": "f32 bulk; f64 z, infiltration, deposited mass, budgets",
                  "error_bar": "<=1e-4 relative L-inf on depth and concentration vs FP64 (tests/test_gpu_mixed.py)"}
 
@@ -389,7 +408,7 @@ def main():
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         try:
-            v, el, th, n = run_cpu_reference(case, 1024, 8, host_threads())
+            v, el, th, n = run_cpu_reference(case, 1024, 150, host_threads())
             cpu = {"value": v, "unit": "cell-steps/s", "cores": th, "kind": "reference",
                    "sample": f"SWEHR.c with its OpenMP pragmas on, 1024x1024 corner of the same domain, "
                              f"first {n} steps, {el:.1f} s"}
@@ -414,13 +433,8 @@ def main():
         B = algo_bytes_f64(S)
         upd_ms = kernel_ms / max(steps_done, 1)
         achieved = B * cells / (upd_ms / 1e3) / 1e9 if upd_ms > 0 else None
-        traffic = None
-        tpath = os.path.join(ROOT, "profiles", "update_f64_traffic.json")
-        if os.path.exists(tpath):
-            try:
-                traffic = json.load(open(tpath)).get("bytes_per_launch_scaled")
-            except Exception:
-                traffic = None
+        tb = profiled_traffic("k_update_tile_f64_fractal1024.md")
+        traffic = tb * cells if tb else None
         line = {
             "metric": "cell-steps/s", "value": value, "unit": "cell-steps/s", "n_gpus": world,
             "steps": steps_done, "warmup": args.warmup, "ms_per_step": elapsed_ms / max(steps_done, 1),
