@@ -13,7 +13,9 @@ larger than L2, so no flush is needed between steps.
 N > 1 (torchrun): every rank advances its own replica of the domain (weak
 scaling, no data-path collective -- independent domains do not exchange
 anything); rank 0 prints the whole-job cell-steps/s from the max over ranks
-of the device-timed region.
+of the device-timed region.  The batched-ensemble leg splits its scenarios
+over the ranks by cell count (strong scaling of a fixed ensemble, again
+without exchange); the CPU baseline and the serving leg run at N = 1 only.
 
 --impl reference: the reference program (SWEHR.c built by oracle/build_ref.py
 with its own OpenMP pragmas on) on a crop of the same domain, all host
@@ -187,23 +189,30 @@ def reference_arm(args, rank: int):
     print(json.dumps(line))
 
 
-def ensemble_leg(args):
+def ensemble_leg(args, ranks):
     """The batched ensemble: scenarios with sides log-uniform in 64..1024
     cells (dx = 1 m, per-scenario fractal seeds, rain U(20,150) mm/h, Manning
     n U(0.02,0.08), 7 classes) resident in one pool and stepped by shared
     persistent launches, in the mixed and in the plain FP64 form; each form's
-    launch shape picked by the pool's tuner first.  Every scenario is capped
-    at the same step count, so after the timed steps both pools hold the
-    same steps of every scenario and a subset is compared field by field
-    (mixed vs FP64, beside FP64 on FP32-rounded inputs: the envelope)."""
+    launch shape picked by the pool's tuner first.  With N ranks the
+    scenarios are split over the GPUs by cell count (no exchange: strong
+    scaling of a fixed ensemble); throughput is all ranks' cell-steps over
+    the slowest rank's device time.  Every scenario is capped at the same
+    step count, so after the timed steps both pools hold the same steps of
+    every scenario and a subset is compared field by field (mixed vs FP64,
+    beside FP64 on FP32-rounded inputs: the envelope)."""
     from swehr_b200.accuracy import rel_linf, quantized_case
     from swehr_b200 import workloads as W
     from swehr_b200.lib import Pool, Simulation
     from swehr_b200.params import FP64, MIXED
-    cases = W.ensemble(args.ens_count)
-    cells = sum(c.cells() for c in cases)
+    from swehr_b200.ranks import shard
+    all_cases = W.ensemble(args.ens_count)
+    mine = shard([c.cells() for c in all_cases], ranks.world)[ranks.rank]
+    cases = [all_cases[k] for k in mine]
+    cells = sum(c.cells() for c in all_cases)
     cap = 64 + args.ens_warmup + args.ens_steps
-    subset = list(range(0, len(cases), max(1, len(cases) // 8)))[:8]
+    every = max(1, len(all_cases) // 8)
+    subset = [i for i, k in enumerate(mine) if k % every == 0 and k // every < 8]
     names = ("h", "totsed", "sed")
     out, keep = {}, {}
     for label, prec in (("fp64", FP64), ("mixed", MIXED)):
@@ -215,44 +224,54 @@ def ensemble_leg(args):
             upload_s = time.perf_counter() - t0
             tu = pool.tune(4)
             pool.run(args.ens_warmup)
+            ranks.barrier()
             st = pool.run(args.ens_steps)
-            v = st.cell_steps / (st.device_ms / 1e3)
+            ranks.barrier()
+            dev_ms = ranks.max(st.device_ms)
+            cs = ranks.sum(st.cell_steps)
             pool.run(-1)
             keep[label] = [scs[k].fields(names) for k in subset]
-            out[label] = {"value": v, "unit": "cell-steps/s", "pool_steps": int(st.pool_steps),
-                          "device_ms": st.device_ms, "ms_per_pool_step": st.device_ms / max(st.pool_steps, 1),
+            out[label] = {"value": cs / (dev_ms / 1e3), "unit": "cell-steps/s", "pool_steps": int(st.pool_steps),
+                          "device_ms": dev_ms, "ms_per_pool_step": dev_ms / max(st.pool_steps, 1),
                           "grid_wave": int(tu.grid_wave), "grid_update": int(tu.grid_update),
-                          "upload_s": upload_s, "hbm_bytes": int(st.hbm_used)}
+                          "upload_s": upload_s, "hbm_bytes_rank0": int(st.hbm_used)}
     # envelope: FP64 on the subset's inputs rounded to FP32
     env = []
-    with Pool(precision=FP64, max_classes=8, max_scenarios=len(subset) + 1) as pool:
-        scs = [pool.submit(quantized_case(cases[k]), max_steps=cap) for k in subset]
-        pool.run(-1)
-        env = [s.fields(names) for s in scs]
+    if subset:
+        with Pool(precision=FP64, max_classes=8, max_scenarios=len(subset) + 1) as pool:
+            scs = [pool.submit(quantized_case(cases[k]), max_steps=cap) for k in subset]
+            pool.run(-1)
+            env = [s.fields(names) for s in scs]
     err = {n: 0.0 for n in names}
     envm = {n: 0.0 for n in names}
     for a, b, q in zip(keep["mixed"], keep["fp64"], env):
         for n in names:
             err[n] = max(err[n], rel_linf(a[n], b[n]))
             envm[n] = max(envm[n], rel_linf(q[n], b[n]))
+    err = {n: ranks.max(v) for n, v in err.items()}
+    envm = {n: ranks.max(v) for n, v in envm.items()}
     # the same scenarios one at a time through the single-domain path (FP64)
     t_dev, cs = 0.0, 0
-    for c in cases[:: max(1, len(cases) // 32)]:
-        with Simulation(c) as sim:
+    step = max(1, len(all_cases) // 32)
+    for k in mine:
+        if k % step:
+            continue
+        with Simulation(all_cases[k]) as sim:
             sim.advance(max_steps=3)
             pr = sim.advance(max_steps=args.ens_solo_steps)
             t_dev += pr.device_ms
-            cs += c.cells() * pr.steps_this_call
-    solo = cs / (t_dev / 1e3)
-    return {"workload": f"{len(cases)} scenarios, sides log-uniform 64..1024 (seed 2), {cells} cells, 7 classes",
-            "scenarios": len(cases), "cells": cells, "steps_per_scenario": cap,
+            cs += all_cases[k].cells() * pr.steps_this_call
+    solo = ranks.sum(cs) / (ranks.sum(t_dev) / 1e3) if ranks.sum(t_dev) > 0 else None
+    return {"workload": f"{len(all_cases)} scenarios, sides log-uniform 64..1024 (seed 2), {cells} cells, 7 classes",
+            "scenarios": len(all_cases), "cells": cells, "steps_per_scenario": cap,
+            "placement": f"split over {ranks.world} GPU(s) by cells, no exchange"
+                         + (" (strong scaling)" if ranks.world > 1 else ""),
             "batched_mixed": out["mixed"], "batched_fp64": out["fp64"],
-            "solo_fp64": {"value": solo, "unit": "cell-steps/s",
-                          "sample": f"every {max(1, len(cases) // 32)}th scenario alone, "
-                                    f"{args.ens_solo_steps} steps each"},
+            "solo_fp64": {"value": solo, "unit": "cell-steps/s per GPU",
+                          "sample": f"every {step}th scenario alone, {args.ens_solo_steps} steps each"},
             "mixed_over_batched_fp64": out["mixed"]["value"] / out["fp64"]["value"],
-            "mixed_over_solo_fp64": out["mixed"]["value"] / solo,
-            "error_vs_fp64": {"scenarios": [int(k) for k in subset], "rel_linf": err,
+            "mixed_over_solo_fp64": (out["mixed"]["value"] / ranks.world / solo) if solo else None,
+            "error_vs_fp64": {"scenarios": [int(k) for k in range(0, len(all_cases), every)][:8], "rel_linf": err,
                               "fp32_input_envelope": envm}}
 
 
@@ -312,34 +331,18 @@ def main():
         reference_arm(args, rank)
         return
 
-    dist = None
     if world > 1:
-        import datetime
         import torch
-        import torch.distributed as dist
         torch.cuda.set_device(0)
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    from swehr_b200.ranks import Ranks
+    ranks = Ranks("nccl", timeout_s=600.0)
+    barrier, max_over_ranks = ranks.barrier, ranks.max
 
     from swehr_b200.lib import Simulation
     from swehr_b200.params import FP64, MIXED
     case = bench_workload(args)
     S = case.sclass
     cells = case.cells()
-
-    def barrier():
-        if dist is not None:
-            import torch
-            t = torch.ones(1, device="cuda")
-            dist.all_reduce(t)
-            torch.cuda.synchronize()
-
-    def max_over_ranks(x: float) -> float:
-        if dist is None:
-            return x
-        import torch
-        t = torch.tensor([x], device="cuda", dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
 
     def timed_run(precision, clocks=None):
         sim = Simulation(case, precision=precision)
@@ -394,12 +397,7 @@ def main():
         s2.close()
         h2d = case.topo.nbytes + (case.ks.nbytes if case.ks is not None else 0) + case.rain.nbytes
         d2h = sum(v.nbytes for v in out.values())
-        e2e_val = cells * (args.warmup + args.steps) / (t1 - t0)
-        if dist is not None:
-            import torch
-            t = torch.tensor([t1 - t0], device="cuda", dtype=torch.float64)
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            e2e_val = world * cells * (args.warmup + args.steps) / float(t.item())
+        e2e_val = world * cells * (args.warmup + args.steps) / max_over_ranks(t1 - t0)
         n_e2e = args.warmup + args.steps
         e2e = {"value": e2e_val, "unit": "cell-steps/s", "h2d_bytes_per_step": h2d / n_e2e,
                "d2h_bytes_per_step": d2h / n_e2e,
@@ -417,11 +415,14 @@ def main():
                    "sample": f"unavailable: {e}"}
 
     ensemble = serving = None
-    if rank == 0 and world == 1 and not args.no_ensemble:
-        try:
-            ensemble = ensemble_leg(args)
-        except Exception as e:  # noqa: BLE001
-            ensemble = {"error": repr(e)}
+    if not args.no_ensemble:
+        if world == 1:
+            try:
+                ensemble = ensemble_leg(args, ranks)
+            except Exception as e:  # noqa: BLE001
+                ensemble = {"error": repr(e)}
+        else:
+            ensemble = ensemble_leg(args, ranks)   # every rank takes the same collective steps
     if rank == 0 and world == 1 and not args.no_serving:
         try:
             serving = serving_leg(args)
@@ -459,9 +460,7 @@ def main():
             "impl": "swehr",
         }
         print(json.dumps(line))
-    if dist is not None:
-        dist.barrier()
-        dist.destroy_process_group()
+    ranks.close()
 
 
 if __name__ == "__main__":
