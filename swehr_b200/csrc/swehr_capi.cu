@@ -192,6 +192,7 @@ static void make_devparams(const swehr_params *p, const swehr_inputs *in, const 
     P.uc = p->uc; P.uc2 = p->uc2; P.cstable = p->cstable; P.maxstep = p->maxstep;
     P.c109s = 1.09 * (p->rhos / p->rhow - 1);
     P.rhos08 = 0.8 * p->rhos;
+    P.inv_rhos = 1.0 / p->rhos;
     P.storm_peak = p->storm_peak; P.storm_r2 = p->storm_radius * p->storm_radius;
     P.storm_x0 = p->storm_x0; P.storm_y0 = p->storm_y0; P.storm_vx = p->storm_vx; P.storm_vy = p->storm_vy;
     for (int k = 0; k < p->sclass; k++) {

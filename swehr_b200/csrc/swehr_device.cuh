@@ -49,6 +49,7 @@ struct DevParams {
     double roughness, ks, theta0, thetas, hf, uc, uc2, cstable, maxstep;
     double c109s;         /* 1.09*(rhos/rhow-1), settlingvelocity (SWEHR.c:433-435) */
     double rhos08;        /* 0.8*rhos */
+    double inv_rhos;      /* 1/rhos (the mixed form's deposited thickness) */
     double storm_peak, storm_r2, storm_x0, storm_y0, storm_vx, storm_vy;
     double ds[16], pf[16], a13[16], a13sq[16];
     RealC<double> kd;     /* the constants above, for templated kernels */

@@ -182,11 +182,29 @@ SW_HD int sw_is_odd_int(double y)
     return (y == (double)k) && (k & 1);
 }
 
+/* x^4 as the square of x^2, both squares carried as double-doubles: the
+ * error before the final rounding is about 2^-104 relative, so the result is
+ * the correctly rounded x^4 unless x^4 lies that close to a rounding
+ * boundary.  Finite x with x^4 in the normal range. */
+SW_HD double sw_pow4(double x)
+{
+    double p = x * x;
+    double e = fma(x, x, -p);                 /* x^2 = p + e exactly */
+    double P = p * p;
+    double lo = fma(p, p, -P);                /* p^2 = P + lo exactly */
+    lo = fma(2.0 * p, e, lo);                 /* + 2 p e; e^2 is below 2^-104 P */
+    return P + lo;
+}
+
 SW_HD double sw_pow(double x, double y)
 {
     if (y == 0.5) return sw_sqrt_pow(x);
     if (y == 1.0) return x;
     if (y == 2.0) return x * x;
+    if (y == 4.0) {
+        double ax4 = x < 0 ? -x : x;
+        if (ax4 >= 0x1p-250 && ax4 <= 0x1p250) return sw_pow4(x);
+    }
     if (y == 0.0 || x == 1.0) return 1.0;
     if (x != x || y != y) return x + y;
     double ax = x < 0 ? -x : x;

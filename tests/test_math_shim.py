@@ -89,3 +89,4 @@ def test_agreement_with_glibc(shim, glibc):
     same_exp = np.mean([shim.orc_m_exp(-float(x) * 50) == glibc.orc_m_exp(-float(x) * 50) for x in xs])
     same_sqrt = np.mean([shim.orc_m_powh(float(x)) == glibc.orc_m_powh(float(x)) for x in xs])
     assert same_pow > 0.99 and same_exp > 0.98 and same_sqrt > 0.99, (same_pow, same_exp, same_sqrt)
+
