@@ -91,3 +91,20 @@ def test_mixed_hillslope_full_run_and_budget():
 @pytest.mark.parametrize("steps", [150, 600])
 def test_mixed_fractal(steps):
     check(W.fractal_domain(nx=256, ny=192, dx=2.0, steps=steps), steps=steps)
+
+
+def test_error_study_small():
+    """The long-run error study on a small storm domain: checkpoints carry
+    every field's error, the envelope, and budget closure of both forms."""
+    from swehr_b200.error_study import run
+    rep = run(nx=192, ny=160, steps=300, every=150, envelope=True)
+    rows = rep["checkpoints"]
+    assert [r["step"] for r in rows] == [150, 300]
+    for r in rows:
+        assert r["steps"]["fp64"] == r["steps"]["mixed"] == r["steps"]["fp64_on_fp32_inputs"] == r["step"]
+        for key in ("h", "totsed", "sed_max", "U_max", "M_max"):
+            assert key in r["rel_linf"] and key in r["envelope"]
+        for name in ("h", "totsed", "sed_max"):
+            bound = TOL if r["envelope"][name] < 1e-5 else max(TOL, 10 * r["envelope"][name])
+            assert r["rel_linf"][name] <= bound, (r["step"], name, r["rel_linf"][name], r["envelope"][name])
+        assert r["budget"]["fp64"]["water"] <= 1e-9 and r["budget"]["mixed"]["water"] <= 1e-6
