@@ -56,6 +56,8 @@ struct BatchConfig {
      * the largest class count among the scenarios is S (index S = 0..16) */
     size_t smem_update_s[17] = {};
     int occ_update_s[17] = {};
+    int stage_m_s[17] = {};             /* stage M_k in shared memory at this class count */
+    void *fn_update_s[17] = {};         /* the update kernel for that choice */
 };
 
 int configure_batch_f64(int max_classes, bool budget, BatchConfig &cfg);
@@ -66,6 +68,7 @@ struct StepConfig {
     int grid_wave = 1, grid_update = 1;
     size_t smem_wave = 0, smem_update = 0;
     void *fn_update = nullptr, *fn_wave = nullptr;
+    int stage_m = 1;                    /* the update stages M_k in shared memory */
 };
 
 /* Pick the kernel instantiations, set their shared-memory limit and size the

@@ -15,31 +15,64 @@ template <class PP, class RS>
 struct FormLauncher {
     typedef typename PP::R R;
 
-    static size_t update_smem(int S) { return StagedLayout::make(S, sizeof(R), 1).total; }
+    static size_t update_smem(int S, int stage_m = 1) { return StagedLayout::make(S, sizeof(R), 1, stage_m).total; }
+
+    /* The update kernel and shared memory for S classes: M_k staged unless
+     * leaving it in global memory fits more blocks per SM (measured: staging
+     * is 2-5 % faster at equal occupancy; at 10 FP64 classes dropping it
+     * doubles the resident blocks and the update runs ~27 % faster).  Sets
+     * both kernels' shared-memory limits. */
+    static cudaError_t pick_staging(void *f_with, void *f_without, int S, size_t &smem, int &occ, int &stage_m,
+                                    void *&fn)
+    {
+        const size_t with = update_smem(S, 1), without = update_smem(S, 0);
+        int ow = 0, oo = 0;
+        cudaError_t e = cudaFuncSetAttribute(f_with, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)with);
+        if (e != cudaSuccess) return e;
+        e = cudaFuncSetAttribute(f_without, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)without);
+        if (e != cudaSuccess) return e;
+        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&ow, f_with, TILE_THREADS, with);
+        if (e != cudaSuccess) return e;
+        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&oo, f_without, TILE_THREADS, without);
+        if (e != cudaSuccess) return e;
+        stage_m = ow >= oo;
+        smem = stage_m ? with : without;
+        occ = stage_m ? ow : oo;
+        fn = stage_m ? f_with : f_without;
+        if (occ < 1) occ = 1;
+        return cudaSuccess;
+    }
     static size_t wave_smem() { return StagedLayout::make(0, sizeof(R), 0).total; }
 
-    template <int MAXS, bool BUDGET>
-    static void *update_fn() { return (void *)k_update_tile<PP, RS, MAXS, BUDGET>; }
+    template <int MAXS, bool BUDGET, bool SM>
+    static void *update_fn() { return (void *)k_update_tile<PP, RS, MAXS, BUDGET, SM>; }
 
-    static void *pick_update(int S, bool budget)
+    template <bool BUDGET, bool SM>
+    static void *pick_u(int S)
     {
-        if (S <= 4) return budget ? update_fn<4, true>() : update_fn<4, false>();
-        if (S <= 8) return budget ? update_fn<8, true>() : update_fn<8, false>();
-        return budget ? update_fn<16, true>() : update_fn<16, false>();
+        if (S <= 4) return update_fn<4, BUDGET, SM>();
+        if (S <= 8) return update_fn<8, BUDGET, SM>();
+        return update_fn<16, BUDGET, SM>();
+    }
+
+    static void *pick_update(int S, bool budget, bool sm)
+    {
+        if (budget) return sm ? pick_u<true, true>(S) : pick_u<true, false>(S);
+        return sm ? pick_u<false, true>(S) : pick_u<false, false>(S);
     }
 
     static int configure(const DevParams &P, int num_sms, StepConfig &cfg)
     {
         const int64_t ntiles = (int64_t)((P.nx + T_I - 1) / T_I) * ((P.ny + T_J - 1) / T_J);
-        void *fu = pick_update(P.S, P.budget != 0);
+        void *fu = nullptr;
         void *fw = (void *)k_wave_tile<PP, RS>;
-        const size_t su = update_smem(P.S), sw = wave_smem();
-        cudaError_t e = cudaFuncSetAttribute(fu, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)su);
+        size_t su = 0;
+        const size_t sw = wave_smem();
+        int occ_u = 0, occ_w = 0, stage_m = 1;
+        cudaError_t e = pick_staging(pick_update(P.S, P.budget != 0, true), pick_update(P.S, P.budget != 0, false),
+                                     P.S, su, occ_u, stage_m, fu);
         if (e != cudaSuccess) return (int)e;
         e = cudaFuncSetAttribute(fw, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sw);
-        if (e != cudaSuccess) return (int)e;
-        int occ_u = 0, occ_w = 0;
-        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_u, fu, TILE_THREADS, su);
         if (e != cudaSuccess) return (int)e;
         e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_w, fw, TILE_THREADS, sw);
         if (e != cudaSuccess) return (int)e;
@@ -51,39 +84,45 @@ struct FormLauncher {
         cfg.smem_wave = sw;
         cfg.fn_update = fu;
         cfg.fn_wave = fw;
+        cfg.stage_m = stage_m;
         return 0;
     }
 
-    template <int MAXS, bool BUDGET>
-    static void *ubatch_fn() { return (void *)k_update_batch<PP, RS, MAXS, BUDGET>; }
+    template <int MAXS, bool BUDGET, bool SM>
+    static void *ubatch_fn() { return (void *)k_update_batch<PP, RS, MAXS, BUDGET, SM>; }
+
+    template <bool SM>
+    static void *pick_ub(int max_classes, bool budget)
+    {
+        if (max_classes <= 4) return budget ? ubatch_fn<4, true, SM>() : ubatch_fn<4, false, SM>();
+        if (max_classes <= 8) return budget ? ubatch_fn<8, true, SM>() : ubatch_fn<8, false, SM>();
+        return budget ? ubatch_fn<16, true, SM>() : ubatch_fn<16, false, SM>();
+    }
 
     static int configure_batch(int max_classes, bool budget, BatchConfig &cfg)
     {
-        void *fu;
-        if (max_classes <= 4) fu = budget ? ubatch_fn<4, true>() : ubatch_fn<4, false>();
-        else if (max_classes <= 8) fu = budget ? ubatch_fn<8, true>() : ubatch_fn<8, false>();
-        else fu = budget ? ubatch_fn<16, true>() : ubatch_fn<16, false>();
+        void *fu_with = pick_ub<true>(max_classes, budget), *fu_without = pick_ub<false>(max_classes, budget);
         void *fw = (void *)k_wave_batch<PP, RS>;
         const size_t su = update_smem(max_classes), sw = wave_smem();
-        cudaError_t e = cudaFuncSetAttribute(fu, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)su);
-        if (e != cudaSuccess) return (int)e;
-        e = cudaFuncSetAttribute(fw, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sw);
-        if (e != cudaSuccess) return (int)e;
-        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&cfg.occ_update, fu, TILE_THREADS, su);
+        cudaError_t e = cudaFuncSetAttribute(fw, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sw);
         if (e != cudaSuccess) return (int)e;
         e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&cfg.occ_wave, fw, TILE_THREADS, sw);
         if (e != cudaSuccess) return (int)e;
-        if (cfg.occ_update < 1) cfg.occ_update = 1;
         if (cfg.occ_wave < 1) cfg.occ_wave = 1;
+        cfg.occ_update = 1;
         for (int S = 0; S <= 16; S++) {
             const int Sc = S < 1 ? 1 : (S > max_classes ? max_classes : S);
-            cfg.smem_update_s[S] = update_smem(Sc);
-            int o = 0;
-            e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o, fu, TILE_THREADS, cfg.smem_update_s[S]);
+            e = pick_staging(fu_with, fu_without, Sc, cfg.smem_update_s[S], cfg.occ_update_s[S], cfg.stage_m_s[S],
+                             cfg.fn_update_s[S]);
             if (e != cudaSuccess) return (int)e;
-            cfg.occ_update_s[S] = o < 1 ? 1 : o;
+            if (cfg.occ_update_s[S] > cfg.occ_update) cfg.occ_update = cfg.occ_update_s[S];
         }
-        cfg.fn_update = fu;
+        /* limits for the largest shape either kernel is launched with */
+        e = cudaFuncSetAttribute(fu_with, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)su);
+        if (e != cudaSuccess) return (int)e;
+        e = cudaFuncSetAttribute(fu_without, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)update_smem(max_classes, 0));
+        if (e != cudaSuccess) return (int)e;
+        cfg.fn_update = cfg.fn_update_s[max_classes];
         cfg.fn_wave = fw;
         cfg.smem_update = su;
         cfg.smem_wave = sw;

@@ -55,10 +55,12 @@ struct swehr_pool {
     int kw_sel = 0, ku_sel = 0;          /* tuned blocks per SM (0: occupancy) */
     int max_s = 1;                       /* largest class count running */
     size_t smem_update = 0;              /* update kernel's dynamic shared memory now */
+    void *fn_update = nullptr;           /* update kernel now (staging choice for max_s) */
     cudaStream_t stream = nullptr;
     struct GraphEntry {
         size_t smem;
         int gw, gu;
+        void *fn;
         cudaGraphExec_t exec;
     };
     std::vector<GraphEntry> graphs;      /* one per launch shape seen (class count x grids) */
@@ -195,8 +197,7 @@ static void launch_pool_step(swehr_pool *pl, cudaEvent_t e0, cudaEvent_t e1, cud
     if (e0) cudaEventRecord(e0, pl->stream);
     cudaLaunchKernel(pl->cfg.fn_wave, dim3(pl->grid_wave), dim3(pl->cfg.threads), args, pl->cfg.smem_wave, pl->stream);
     if (e1) cudaEventRecord(e1, pl->stream);
-    cudaLaunchKernel(pl->cfg.fn_update, dim3(pl->grid_update), dim3(pl->cfg.threads), args, pl->smem_update,
-                     pl->stream);
+    cudaLaunchKernel(pl->fn_update, dim3(pl->grid_update), dim3(pl->cfg.threads), args, pl->smem_update, pl->stream);
     if (e2) cudaEventRecord(e2, pl->stream);
 }
 
@@ -207,7 +208,7 @@ static void launch_pool_step(swehr_pool *pl, cudaEvent_t e0, cudaEvent_t e1, cud
 static int pool_graph(swehr_pool *pl, cudaGraphExec_t *out)
 {
     for (auto &g : pl->graphs)
-        if (g.smem == pl->smem_update && g.gw == pl->grid_wave && g.gu == pl->grid_update) {
+        if (g.smem == pl->smem_update && g.gw == pl->grid_wave && g.gu == pl->grid_update && g.fn == pl->fn_update) {
             *out = g.exec;
             return SWEHR_OK;
         }
@@ -219,7 +220,7 @@ static int pool_graph(swehr_pool *pl, cudaGraphExec_t *out)
     cudaError_t e = cudaGraphInstantiate(&ex, g, 0);
     cudaGraphDestroy(g);
     if (e != cudaSuccess) return swehr_err(SWEHR_CUDA_ERROR, std::string("cudaGraphInstantiate: ") + cudaGetErrorString(e));
-    pl->graphs.push_back({pl->smem_update, pl->grid_wave, pl->grid_update, ex});
+    pl->graphs.push_back({pl->smem_update, pl->grid_wave, pl->grid_update, pl->fn_update, ex});
     *out = ex;
     return SWEHR_OK;
 }
@@ -237,6 +238,7 @@ static void set_grids(swehr_pool *pl, int kw, int ku)
 static void apply_shape(swehr_pool *pl)
 {
     pl->smem_update = pl->cfg.smem_update_s[pl->max_s];
+    pl->fn_update = pl->cfg.fn_update_s[pl->max_s];
     const int occ_u = pl->cfg.occ_update_s[pl->max_s];
     const int ku = pl->ku_sel ? std::min(pl->ku_sel, occ_u) : occ_u;
     const int kw = pl->kw_sel ? pl->kw_sel : pl->cfg.occ_wave;

@@ -217,14 +217,19 @@ struct StagedLayout {
     /* byte offsets from the start of dynamic shared memory */
     size_t halo, cell_r, cell_d, zp, zc, u, v, g, c, sed, fx, fy, up, red, total;
     int nhalo, ncellr, ncelld;
-    __host__ __device__ static StagedLayout make(int S, size_t rs, int what)
+    int stage_m;          /* M_k staged here (else read from global memory by the cell stage) */
+    /* stage_m: staging M_k costs 2 KB of shared memory per class; the
+     * launcher picks the kernel that stages it only where that costs no
+     * resident blocks (a compile-time choice of each kernel) */
+    __host__ __device__ static StagedLayout make(int S, size_t rs, int what, int stage_m = 1)
     {
         StagedLayout L;
         size_t o = 0;
         auto take = [&](size_t bytes) { size_t at = o; o += (bytes + 15) / 16 * 16; return at; };
+        L.stage_m = what && stage_m;
         L.nhalo = what ? 5 + S : 3;
         L.ncellr = what ? 4 : 0;
-        L.ncelld = what ? 1 + S : 0;
+        L.ncelld = what ? (L.stage_m ? 1 + S : 1) : 0;
         L.halo = take((size_t)L.nhalo * HALO_ROWS * R_J * rs);
         L.cell_r = take((size_t)L.ncellr * T_I * T_J * rs);
         L.cell_d = take((size_t)L.ncelld * T_I * T_J * sizeof(double));
@@ -332,8 +337,10 @@ __device__ __forceinline__ void stage_load(const DevParams &P, const SetV<RS> &s
                 cp_pair(cr + CR_MAXDEP * ps, src.maxdep + go);
                 if (P.has_ks) cp_pair(cr + CR_KS * ps, ks + go);
                 cp_pair(cd + CD_VINF * ps, src.vinf + go);
-                const double *m = src.M + go;
-                for (int k = 0; k < P.S; k++) cp_pair(cd + (CD_M + k) * ps, m + (int64_t)k * pl);
+                if (L.stage_m) {
+                    const double *m = src.M + go;
+                    for (int k = 0; k < P.S; k++) cp_pair(cd + (CD_M + k) * ps, m + (int64_t)k * pl);
+                }
             }
         }
     }
@@ -762,7 +769,7 @@ __device__ __forceinline__ void tile_cell(const DevParams &P, const SetV<RS> &sr
     for (int k = 0; k < MAXS; k++) {
         if (k >= S) break;
         const int64_t qm = k * pl + q;
-        const double Mk0 = celld[(CD_M + k) * T_I * T_J + cs];
+        const double Mk0 = L.stage_m ? celld[(CD_M + k) * T_I * T_J + cs] : __ldg(src.M + qm);
         const R Mk0r = (R)Mk0;
         R E1 = 0, E2 = 0, E3 = 0, E4 = 0;
         if (swash) {
@@ -1085,7 +1092,7 @@ __device__ __forceinline__ void budget_fold(Ctl *ctl, int m, double hi, double l
     ctl->budget_lo[m] = Ll;
 }
 
-template <class PP, class RS, int MAXS, bool BUDGET>
+template <class PP, class RS, int MAXS, bool BUDGET, bool STAGE_M>
 __global__ void __launch_bounds__(TILE_THREADS, PP::kMinBlocks) k_update_tile(const DevParams P, const BufsT<RS> B, Ctl *ctl,
                                                                   const double *__restrict__ rain, double *partials,
                                                                   double *stage, double *saveflow)
@@ -1094,7 +1101,7 @@ __global__ void __launch_bounds__(TILE_THREADS, PP::kMinBlocks) k_update_tile(co
     if (!ctl->pending) return;
     extern __shared__ __align__(16) unsigned char smb[];
     __shared__ bool last;
-    const StagedLayout L = StagedLayout::make(P.S, sizeof(R), 1);
+    const StagedLayout L = StagedLayout::make(P.S, sizeof(R), 1, STAGE_M);
     const int64_t n = ctl->step;
     const double t = ctl->t, dt = ctl->dt;
     const double Rr = P.storm ? 0.0 : rain_at(P, rain, t);
@@ -1191,7 +1198,7 @@ __global__ void __launch_bounds__(TILE_THREADS) k_wave_batch(const BatchHdr<RS> 
     }
 }
 
-template <class PP, class RS, int MAXS, bool BUDGET>
+template <class PP, class RS, int MAXS, bool BUDGET, bool STAGE_M>
 __global__ void __launch_bounds__(TILE_THREADS, PP::kMinBlocks) k_update_batch(const BatchHdr<RS> *__restrict__ hdr)
 {
     typedef typename PP::R R;
@@ -1210,7 +1217,7 @@ __global__ void __launch_bounds__(TILE_THREADS, PP::kMinBlocks) k_update_batch(c
         const ScenDesc<RS> &D = sd;
         Ctl *ctl = D.ctl;
         if (!ctl->pending) continue;
-        const StagedLayout L = StagedLayout::make(D.P.S, sizeof(R), 1);
+        const StagedLayout L = StagedLayout::make(D.P.S, sizeof(R), 1, STAGE_M);
         const int64_t n = ctl->step;
         const double t = ctl->t, dt = ctl->dt, Rr = ctl->rain_now;
         Acc2<MAXS, BUDGET> acc;
