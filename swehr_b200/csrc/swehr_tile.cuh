@@ -1143,23 +1143,42 @@ __global__ void __launch_bounds__(TILE_THREADS, PP::kMinBlocks) k_update_tile(co
  * arithmetic, so every scenario's result is identical alone or in a batch.
  * Budget sums of a batched step are block partials added with atomics
  * (order-dependent rounding of the budget terms only). */
-/* Copy scenario sid's descriptor into the block's shared copy unless it is
- * already there (the whole block calls it; sid is uniform).  Parameters then
- * come from a shared object no other store can alias, instead of global
- * memory the compiler would have to re-read after every store. */
+/* Copy scenario sid's descriptor into the block's shared copy (the whole
+ * block calls it).  Parameters then come from a shared object no other store
+ * can alias, instead of global memory the compiler would have to re-read
+ * after every store.  Thread 0 also snapshots the scenario's step state: it
+ * cannot change while this block still holds uncounted tiles of it (the
+ * scenario's pass ends only once every tile is counted). */
+struct StepSnap {
+    double t, dt, rain;
+    int64_t n;
+    int32_t go;                          /* active (wave pass) / pending (update pass) */
+};
+
 template <class RS>
-__device__ __forceinline__ void load_desc(const ScenDesc<RS> *tab, int sid, ScenDesc<RS> &sd, int &cur)
+__device__ __forceinline__ void load_desc(const ScenDesc<RS> *tab, int sid, ScenDesc<RS> &sd, StepSnap &snap,
+                                          bool update_pass)
 {
-    if (sid == cur) return;
     static_assert(sizeof(ScenDesc<RS>) % 8 == 0, "descriptor copied in 8-byte words");
     const unsigned long long *src = reinterpret_cast<const unsigned long long *>(tab + sid);
     unsigned long long *dst = reinterpret_cast<unsigned long long *>(&sd);
-    __syncthreads();                                             /* previous tile is done with sd */
+    __syncthreads();                                             /* the previous run is done with sd */
     for (int w = threadIdx.x; w < (int)(sizeof(ScenDesc<RS>) / 8); w += blockDim.x) dst[w] = src[w];
+    if (threadIdx.x == 0) {
+        const Ctl *ctl = tab[sid].ctl;
+        snap.go = update_pass ? ctl->pending : ctl->active;
+        snap.n = ctl->step;
+        snap.t = ctl->t;
+        snap.dt = ctl->dt;
+        snap.rain = ctl->rain_now;
+    }
     __syncthreads();
-    cur = sid;
 }
 
+/* Batched wave pass.  A block walks the tile list with a grid stride and
+ * keeps a run per scenario: consecutive tiles of one scenario share the
+ * descriptor copy and a running max, and the scenario's ticket is advanced
+ * by the run's tile count once, when the block moves on (or finishes). */
 template <class PP, class RS>
 __global__ void __launch_bounds__(TILE_THREADS) k_wave_batch(const BatchHdr<RS> *__restrict__ hdr)
 {
@@ -1167,37 +1186,50 @@ __global__ void __launch_bounds__(TILE_THREADS) k_wave_batch(const BatchHdr<RS> 
     extern __shared__ __align__(16) unsigned char smb[];
     __shared__ double red8[TILE_THREADS / 32];
     __shared__ __align__(16) ScenDesc<RS> sd;
+    __shared__ StepSnap snap;
     const StagedLayout L = StagedLayout::make(0, sizeof(R), 0);
     const ScenDesc<RS> *tab = hdr->tab;
     const int32_t *map = hdr->tile_scen;
     const int64_t total = hdr->total_tiles;
     int cur = -1;
+    unsigned run = 0;                    /* tiles of `cur` done and not yet counted */
+    R smax = 0;
+    auto flush = [&]() {
+        const double m = block_max((double)smax, red8);
+        if (threadIdx.x == 0) {
+            Ctl *ctl = sd.ctl;
+            atomicMax(&ctl->smax_bits, (unsigned long long)__double_as_longlong(m));
+            __threadfence();
+            if (atomicAdd(&ctl->wave_ticket, run) == (unsigned)sd.ntiles - run) {
+                wave_finalize(sd.P, ctl);
+                /* the step's uniform rain rate, read by every update tile */
+                ctl->rain_now = sd.P.storm ? 0.0 : rain_at(sd.P, sd.rain, snap.t);
+            }
+        }
+        run = 0;
+        smax = 0;
+    };
     int sid_next = blockIdx.x < total ? map[blockIdx.x] : 0;
     for (int64_t g = blockIdx.x; g < total; g += gridDim.x) {
         const int sid = sid_next;                                /* uniform across the block */
         if (g + gridDim.x < total) sid_next = map[g + gridDim.x];
-        load_desc(tab, sid, sd, cur);
-        const ScenDesc<RS> &D = sd;
-        Ctl *ctl = D.ctl;
-        if (!ctl->active) continue;
-        const int64_t n = ctl->step;
-        const double t = ctl->t;
-        const R s = wave_tile<PP, RS>(D.P, D.B.set[n & 1], D.B.z[(n + 2) % 3], tile_coord(D.P, g - D.tile0), smb, L,
-                                      t);
-        const double m = block_max((double)s, red8);
-        if (threadIdx.x == 0) {
-            atomicMax(&ctl->smax_bits, (unsigned long long)__double_as_longlong(m));
-            __threadfence();
-            if (atomicAdd(&ctl->wave_ticket, 1u) == (unsigned)(D.ntiles - 1)) {
-                wave_finalize(D.P, ctl);
-                /* the step's uniform rain rate, read by every update tile */
-                ctl->rain_now = D.P.storm ? 0.0 : rain_at(D.P, D.rain, t);
-            }
+        if (sid != cur) {
+            if (run) flush();
+            load_desc(tab, sid, sd, snap, false);
+            cur = sid;
         }
-        __syncthreads();
+        if (!snap.go) continue;
+        const int64_t n = snap.n;
+        const R s = wave_tile<PP, RS>(sd.P, sd.B.set[n & 1], sd.B.z[(n + 2) % 3], tile_coord(sd.P, g - sd.tile0),
+                                      smb, L, snap.t);
+        smax = (s > smax) ? s : smax;
+        run++;
     }
+    if (run) flush();
 }
 
+/* Batched update pass, with the same per-scenario runs: budget accumulators
+ * carry across a run and are summed, counted and folded once per run. */
 template <class PP, class RS, int MAXS, bool BUDGET, bool STAGE_M>
 __global__ void __launch_bounds__(TILE_THREADS, PP::kMinBlocks) k_update_batch(const BatchHdr<RS> *__restrict__ hdr)
 {
@@ -1205,36 +1237,29 @@ __global__ void __launch_bounds__(TILE_THREADS, PP::kMinBlocks) k_update_batch(c
     extern __shared__ __align__(16) unsigned char smb[];
     __shared__ bool last;
     __shared__ __align__(16) ScenDesc<RS> sd;
+    __shared__ StepSnap snap;
     const ScenDesc<RS> *tab = hdr->tab;
     const int32_t *map = hdr->tile_scen;
     const int64_t total = hdr->total_tiles;
     int cur = -1;
-    int sid_next = blockIdx.x < total ? map[blockIdx.x] : 0;
-    for (int64_t g = blockIdx.x; g < total; g += gridDim.x) {
-        const int sid = sid_next;                                /* uniform across the block */
-        if (g + gridDim.x < total) sid_next = map[g + gridDim.x];
-        load_desc(tab, sid, sd, cur);
-        const ScenDesc<RS> &D = sd;
-        Ctl *ctl = D.ctl;
-        if (!ctl->pending) continue;
-        const StagedLayout L = StagedLayout::make(D.P.S, sizeof(R), 1, STAGE_M);
-        const int64_t n = ctl->step;
-        const double t = ctl->t, dt = ctl->dt, Rr = ctl->rain_now;
-        Acc2<MAXS, BUDGET> acc;
-        acc_zero(acc);
-        update_tile<PP, RS, MAXS, BUDGET>(D.P, D.B, n, t, dt, Rr, tile_coord(D.P, g - D.tile0), smb, L, acc);
+    unsigned run = 0;
+    Acc2<MAXS, BUDGET> acc;
+    acc_zero(acc);
+    StagedLayout L = StagedLayout::make(1, sizeof(R), 1, STAGE_M);
+    auto flush = [&]() {
+        Ctl *ctl = sd.ctl;
         double *red = reinterpret_cast<double *>(smb + L.red);
-        const bool bud = BUDGET && D.P.budget;
+        const bool bud = BUDGET && sd.P.budget;
         if (bud) budget_block_sum(acc, red);
         __syncthreads();
-        /* release this tile's writes, count it; the scenario's last tile
-         * acquires everyone's writes before finalizing (one thread fences
-         * on either side of the barrier) */
+        /* release the run's writes, count its tiles; the scenario's last run
+         * acquires everyone's writes before finalizing (one thread fences on
+         * either side of the barrier) */
         if (threadIdx.x == 0) {
             if (bud)
                 for (int m = 0; m < B_NTERMS; m++) atomicAdd(&ctl->budget_step[m], red[m]);
             __threadfence();
-            const bool l = atomicAdd(&ctl->update_ticket, 1u) == (unsigned)(D.ntiles - 1);
+            const bool l = atomicAdd(&ctl->update_ticket, run) == (unsigned)sd.ntiles - run;
             if (l) __threadfence();
             last = l;
         }
@@ -1245,15 +1270,32 @@ __global__ void __launch_bounds__(TILE_THREADS, PP::kMinBlocks) k_update_batch(c
                 ctl->budget_step[threadIdx.x] = 0.0;
                 budget_fold(ctl, threadIdx.x, v, 0.0);
             }
-            update_finalize<PP, RS>(D.P, D.B.set[(n + 1) & 1], ctl, D.stage, D.saveflow, smb);
+            update_finalize<PP, RS>(sd.P, sd.B.set[(snap.n + 1) & 1], ctl, sd.stage, sd.saveflow, smb);
             if (threadIdx.x == 0) {
-                ScenSummary *q = D.sum;
+                ScenSummary *q = sd.sum;
                 q->t = ctl->t; q->dt = ctl->dt; q->courant = ctl->courant; q->step = ctl->step;
                 q->status = ctl->status; q->active = ctl->active;
             }
         }
-        __syncthreads();
+        run = 0;
+        acc_zero(acc);
+    };
+    int sid_next = blockIdx.x < total ? map[blockIdx.x] : 0;
+    for (int64_t g = blockIdx.x; g < total; g += gridDim.x) {
+        const int sid = sid_next;                                /* uniform across the block */
+        if (g + gridDim.x < total) sid_next = map[g + gridDim.x];
+        if (sid != cur) {
+            if (run) flush();
+            load_desc(tab, sid, sd, snap, true);
+            cur = sid;
+            L = StagedLayout::make(sd.P.S, sizeof(R), 1, STAGE_M);
+        }
+        if (!snap.go) continue;
+        update_tile<PP, RS, MAXS, BUDGET>(sd.P, sd.B, snap.n, snap.t, snap.dt, snap.rain,
+                                          tile_coord(sd.P, g - sd.tile0), smb, L, acc);
+        run++;
     }
+    if (run) flush();
 }
 
 }  // namespace swehr
