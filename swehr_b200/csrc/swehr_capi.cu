@@ -280,23 +280,31 @@ static void destroy_ctx(swehr_ctx *c)
     if (c->ev_stop) cudaEventDestroy(c->ev_stop);
     for (int e = 0; e < 2 * TIMING_RING; e++)
         if (c->ev_k[e]) cudaEventDestroy(c->ev_k[e]);
-    if (c->mem) cudaFree(c->mem);
-    if (c->h_ctl) cudaFreeHost(c->h_ctl);
-    if (c->stream) cudaStreamDestroy(c->stream);
+    if (c->host) {
+        if (c->mem) c->host->release(c->host->self, c->mem);
+        free(c->h_ctl);
+    } else {
+        if (c->mem) cudaFree(c->mem);
+        if (c->h_ctl) cudaFreeHost(c->h_ctl);
+        if (c->stream) cudaStreamDestroy(c->stream);
+    }
     delete c;
 }
 
 extern "C" int swehr_create(const swehr_params *p, const swehr_inputs *in, int precision, swehr_ctx **out)
 {
-    return swehr_ctx_create(p, in, precision, 0, out);
+    return swehr_ctx_create(p, in, precision, nullptr, out);
 }
 
 size_t swehr_ctx_footprint(const swehr_params *p, int has_ks, int precision, int num_sms)
 {
-    return layout_for(p->nx, p->ny, p->sclass, p->rnum, has_ks, stagecap_for(p), num_sms * 4, precision).total;
+    /* num_sms 0: a pooled context (one reduction slot; pools sum with atomics) */
+    const int grid = num_sms > 0 ? num_sms * 4 : 1;
+    return layout_for(p->nx, p->ny, p->sclass, p->rnum, has_ks, stagecap_for(p), grid, precision).total;
 }
 
-int swehr_ctx_create(const swehr_params *p, const swehr_inputs *in, int precision, int pooled, swehr_ctx **out)
+int swehr_ctx_create(const swehr_params *p, const swehr_inputs *in, int precision, const CtxHost *host,
+                     swehr_ctx **out)
 {
     if (!out) return set_err(SWEHR_INVALID, "NULL out");
     *out = nullptr;
@@ -308,7 +316,9 @@ int swehr_ctx_create(const swehr_params *p, const swehr_inputs *in, int precisio
     swehr_ctx *c = new swehr_ctx();
     c->p = *p;
     c->precision = precision;
-    c->pooled = pooled;
+    c->pooled = host != nullptr;
+    c->host = host;
+    const int pooled = c->pooled;
     int rc;
 #define CKC(call)                                                                               \
     do {                                                                                        \
@@ -326,7 +336,7 @@ int swehr_ctx_create(const swehr_params *p, const swehr_inputs *in, int precisio
     DevParams tmpP;
     Layout L0 = layout_for(p->nx, p->ny, p->sclass, p->rnum, in->ks != nullptr, c->stagecap, 1, precision);
     make_devparams(p, in, L0, tmpP);
-    {
+    if (!pooled) {
         int ce = precision == SWEHR_MIXED ? configure_step_f32(tmpP, c->num_sms, c->cfg)
                                           : configure_step_f64(tmpP, c->num_sms, c->cfg);
         if (ce) {
@@ -339,8 +349,18 @@ int swehr_ctx_create(const swehr_params *p, const swehr_inputs *in, int precisio
                           precision);
     c->rsize = L.rsize;
     make_devparams(p, in, L, c->P);
-    CKC(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
-    CKC(cudaMalloc((void **)&c->mem, L.total));
+    if (pooled) {
+        c->stream = host->stream;
+        c->mem = (char *)host->alloc(host->self, L.total);
+        if (!c->mem) {
+            rc = set_err(SWEHR_OOM, "scenario allocation failed");
+            destroy_ctx(c);
+            return rc;
+        }
+    } else {
+        CKC(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
+        CKC(cudaMalloc((void **)&c->mem, L.total));
+    }
     c->mem_bytes = L.total;
     CKC(cudaMemsetAsync(c->mem, 0, L.total, c->stream));
     if (precision == SWEHR_MIXED) set_views(c->B32, c->mem, L, p->sclass, in->ks != nullptr, 1);
@@ -350,9 +370,20 @@ int swehr_ctx_create(const swehr_params *p, const swehr_inputs *in, int precisio
     c->d_partials = (double *)(c->mem + L.off_partials);
     c->d_stage = (double *)(c->mem + L.off_stage);
     c->d_saveflow = (double *)(c->mem + L.off_saveflow);
-    CKC(cudaMallocHost((void **)&c->h_ctl, sizeof(Ctl)));
-    CKC(cudaEventCreate(&c->ev_start));
-    CKC(cudaEventCreate(&c->ev_stop));
+    if (pooled) {
+        c->h_ctl = (Ctl *)calloc(1, sizeof(Ctl));
+        if (!c->h_ctl) {
+            rc = set_err(SWEHR_OOM, "host allocation failed");
+            destroy_ctx(c);
+            return rc;
+        }
+    } else {
+        CKC(cudaMallocHost((void **)&c->h_ctl, sizeof(Ctl)));
+    }
+    if (!pooled) {
+        CKC(cudaEventCreate(&c->ev_start));
+        CKC(cudaEventCreate(&c->ev_stop));
+    }
     if (!pooled)
         for (int e = 0; e < 2 * TIMING_RING; e++) CKC(cudaEventCreate(&c->ev_k[e]));
     /* initial state (initialcondition, SWEHR.c:211-285): dry bed, VINF = vinf0, z = topo;

@@ -13,11 +13,23 @@
 static const int GRAPH_STEPS = 32;
 static const int TIMING_RING = 64;
 
+/* What a pool lends the contexts it creates: its stream and a device-memory
+ * allocator (a cache of released allocations), so that admitting and
+ * releasing a scenario needs no cudaMalloc / cudaFree (which synchronises
+ * the device), no stream and no pinned allocation. */
+struct CtxHost {
+    cudaStream_t stream;
+    void *self;
+    void *(*alloc)(void *self, size_t bytes);
+    void (*release)(void *self, void *ptr);
+};
+
 struct swehr_ctx {
     swehr_params p;
     int precision = SWEHR_FP64;
     int device = 0, num_sms = 148;
     int pooled = 0;         /* stepped by a swehr_pool, not by swehr_advance */
+    const CtxHost *host = nullptr;   /* the pool's stream and allocator (pooled contexts) */
     swehr::DevParams P;
     swehr::BufsT<double> B64;      /* plain form */
     swehr::BufsT<float> B32;       /* mixed form */
@@ -41,10 +53,14 @@ struct swehr_ctx {
 /* record an error message for swehr_last_error() and return code */
 int swehr_err(int code, const std::string &msg);
 
-/* Create a context; pooled contexts skip the single-domain timing events. */
-int swehr_ctx_create(const swehr_params *p, const swehr_inputs *in, int precision, int pooled, swehr_ctx **out);
+/* Create a context.  With a host (a pool): stream and device memory come
+ * from it, the control-block mirror is pageable, and the single-domain
+ * kernels are neither configured nor timed. */
+int swehr_ctx_create(const swehr_params *p, const swehr_inputs *in, int precision, const CtxHost *host,
+                     swehr_ctx **out);
 
-/* device bytes swehr_ctx_create() allocates for these inputs (upper bound) */
+/* device bytes swehr_ctx_create() allocates for these inputs (upper bound);
+ * num_sms 0 for a pooled context */
 size_t swehr_ctx_footprint(const swehr_params *p, int has_ks, int precision, int num_sms);
 
 /* free a context (pools use this for their scenarios) */

@@ -19,6 +19,8 @@
 
 #include <algorithm>
 #include <climits>
+#include <map>
+#include <unordered_map>
 #include <cmath>
 #include <cstring>
 #include <string>
@@ -74,6 +76,13 @@ struct swehr_pool {
     int64_t map_cap = 0;
     std::vector<PoolScen> scen;
     std::vector<int> free_slots;
+    /* device memory of scenarios: released allocations are kept for reuse
+     * (within the HBM limit), so admission and release call no cudaMalloc /
+     * cudaFree on the steady path */
+    CtxHost host;
+    std::multimap<size_t, char *> cache;          /* size -> released block */
+    std::unordered_map<char *, size_t> block_size; /* every block the pool owns */
+    size_t cached_bytes = 0;
     int next_id = 1;
     bool dirty = true;
     int nrun = 0;
@@ -88,12 +97,70 @@ struct swehr_pool {
                              std::string(#call) + ": " + cudaGetErrorString(e_));                     \
     } while (0)
 
+static const size_t kBlockGrain = (size_t)2 << 20;
+
+/* keep resident + cached within the HBM limit: drop the largest cached blocks */
+static void trim_cache(swehr_pool *pl, size_t incoming)
+{
+    while (!pl->cache.empty() && pl->hbm_used + pl->cached_bytes + incoming > pl->hbm_limit) {
+        auto it = std::prev(pl->cache.end());
+        cudaFree(it->second);
+        pl->block_size.erase(it->second);
+        pl->cached_bytes -= it->first;
+        pl->cache.erase(it);
+    }
+}
+
+/* a scenario's device memory: the smallest cached block of at least `bytes`
+ * (and at most a quarter more), else a new one */
+static void *pool_alloc(void *self, size_t bytes)
+{
+    swehr_pool *pl = (swehr_pool *)self;
+    const size_t want = (bytes + kBlockGrain - 1) / kBlockGrain * kBlockGrain;
+    auto it = pl->cache.lower_bound(want);
+    if (it != pl->cache.end() && it->first <= want + want / 4) {
+        char *p = it->second;
+        pl->cached_bytes -= it->first;
+        pl->cache.erase(it);
+        return p;
+    }
+    trim_cache(pl, want);                /* room for a new block within the limit */
+    char *p = nullptr;
+    if (cudaMalloc((void **)&p, want) != cudaSuccess) {
+        cudaGetLastError();
+        for (auto &c : pl->cache) {          /* give the cache back and retry once */
+            cudaFree(c.second);
+            pl->block_size.erase(c.second);
+        }
+        pl->cache.clear();
+        pl->cached_bytes = 0;
+        if (cudaMalloc((void **)&p, want) != cudaSuccess) {
+            cudaGetLastError();
+            return nullptr;
+        }
+    }
+    pl->block_size[p] = want;
+    return p;
+}
+
+static void pool_release_block(void *self, void *ptr)
+{
+    swehr_pool *pl = (swehr_pool *)self;
+    char *p = (char *)ptr;
+    auto it = pl->block_size.find(p);
+    if (it == pl->block_size.end()) return;
+    pl->cache.insert({it->second, p});
+    pl->cached_bytes += it->second;
+}
+
 static void pool_free(swehr_pool *pl)
 {
     if (!pl) return;
     if (pl->stream) cudaStreamSynchronize(pl->stream);
     for (auto &s : pl->scen) swehr_ctx_destroy(s.ctx);
     pl->scen.clear();
+    for (auto &c : pl->cache) cudaFree(c.second);
+    pl->cache.clear();
     for (auto &g : pl->graphs) cudaGraphExecDestroy(g.exec);
     if (pl->ev0) cudaEventDestroy(pl->ev0);
     if (pl->ev1) cudaEventDestroy(pl->ev1);
@@ -326,6 +393,10 @@ int swehr_pool_create(int precision, int max_classes, int budget, size_t hbm_lim
         }
     }
     PCKF(cudaStreamCreateWithFlags(&pl->stream, cudaStreamNonBlocking));
+    pl->host.stream = pl->stream;
+    pl->host.self = pl;
+    pl->host.alloc = pool_alloc;
+    pl->host.release = pool_release_block;
     PCKF(cudaEventCreate(&pl->ev0));
     PCKF(cudaEventCreate(&pl->ev1));
     PCKF(cudaMalloc((void **)&pl->d_hdr, 256));
@@ -358,12 +429,15 @@ int swehr_pool_submit(swehr_pool *pl, const swehr_params *p, const swehr_inputs 
     if (p->sclass > pl->max_classes) return swehr_err(SWEHR_INVALID, "sclass above the pool's max_classes");
     if (p->budget && !pl->budget) return swehr_err(SWEHR_INVALID, "pool created without budgets");
     if (p->nx < 2 || p->ny < 2 || p->sclass < 1) return swehr_err(SWEHR_INVALID, "nx, ny >= 2 and sclass >= 1 required");
-    const size_t bytes = swehr_ctx_footprint(p, in->ks != nullptr, pl->precision, pl->num_sms);
+    /* admission by the largest block this scenario can occupy (grain, reuse slack) */
+    const size_t fp = swehr_ctx_footprint(p, in->ks != nullptr, pl->precision, 0);
+    const size_t want = (fp + kBlockGrain - 1) / kBlockGrain * kBlockGrain;
+    const size_t bytes = want + want / 4;
     if (bytes > pl->hbm_limit) return swehr_err(SWEHR_INVALID, "scenario footprint exceeds the pool's HBM limit");
     if (pl->free_slots.empty()) return swehr_err(SWEHR_BUSY, "no free scenario slot");
     if (pl->hbm_used + bytes > pl->hbm_limit) return swehr_err(SWEHR_BUSY, "HBM limit reached");
     swehr_ctx *c = nullptr;
-    int rc = swehr_ctx_create(p, in, pl->precision, 1, &c);
+    int rc = swehr_ctx_create(p, in, pl->precision, &pl->host, &c);
     if (rc) return rc;
     /* arm the control block: active from the first pool step on */
     Ctl *h = c->h_ctl;
@@ -380,7 +454,7 @@ int swehr_pool_submit(swehr_pool *pl, const swehr_params *p, const swehr_inputs 
     PoolScen s;
     s.id = pl->next_id++;
     s.ctx = c;
-    s.bytes = bytes;
+    s.bytes = pl->block_size.count(c->mem) ? pl->block_size[c->mem] : bytes;   /* what it holds */
     s.ntiles = tiles_of(c->P, pl->cfg);
     s.cells = (int64_t)p->nx * p->ny;
     s.slot = pl->free_slots.back();
@@ -398,7 +472,7 @@ int swehr_pool_submit(swehr_pool *pl, const swehr_params *p, const swehr_inputs 
         swehr_ctx_destroy(c);
         return swehr_err(SWEHR_CUDA_ERROR, std::string("summary: ") + cudaGetErrorString(e));
     }
-    pl->hbm_used += bytes;
+    pl->hbm_used += s.bytes;
     pl->scen.push_back(s);
     pl->dirty = true;
     *id = s.id;

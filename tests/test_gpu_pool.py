@@ -142,13 +142,15 @@ def test_pool_budget_closes():
 
 
 def test_pool_admission_by_footprint_and_slots():
-    from swehr_b200.lib import Pool, load
-    L = load()
+    from swehr_b200.lib import Pool
     cases = _cases()
     big = cases[5]
-    fp = L.swehr_footprint_bytes(big.nx, big.ny, big.sclass, FP64)
+    with Pool(precision=FP64, max_classes=8) as pool:
+        pool.submit(big)
+        held = pool.stats().hbm_used          # device bytes one such scenario holds
+    assert held > 0
     # room for one large scenario only
-    with Pool(precision=FP64, max_classes=8, hbm_limit=int(fp * 1.5), max_scenarios=8) as pool:
+    with Pool(precision=FP64, max_classes=8, hbm_limit=int(held * 1.5), max_scenarios=8) as pool:
         a = pool.submit(big)
         assert a is not None
         assert pool.submit(big) is None            # footprint: busy, nothing allocated
@@ -157,8 +159,9 @@ def test_pool_admission_by_footprint_and_slots():
         pool.run(-1)
         assert a.progress().done
         pool.release(a)
-        b = pool.submit(big)                        # memory freed: admitted
+        b = pool.submit(big)                        # memory freed: admitted, its block reused
         assert b is not None
+        assert pool.stats().hbm_used == held
     with Pool(precision=FP64, max_classes=8, max_scenarios=2) as pool:
         assert pool.submit(cases[0]) is not None
         assert pool.submit(cases[1]) is not None
