@@ -276,12 +276,19 @@ def ensemble_leg(args, ranks):
 
 
 def serving_leg(args):
-    """A Poisson request stream through the continuous-batching server."""
+    """A Poisson request stream through the continuous-batching server.  The
+    default stream is scaled to what one B200 serves in real time; with
+    --serve-full it is the full stream (sides to 2048, up to 10 hyetograph
+    steps, 50/s for 60 s), which offers far more work than one GPU does and
+    is reported by its served fraction."""
     from swehr_b200 import serving as SV
     from swehr_b200.params import MIXED
+    if args.serve_full:
+        args.serve_side_max, args.serve_hyeto_max = 2048, 10
+        args.serve_duration, args.serve_drain = 60.0, 60.0
     reqs = SV.poisson_stream(rate=args.serve_rate, duration=args.serve_duration, seed=3, side_min=32,
                              side_max=args.serve_side_max, hyeto_steps=(1, args.serve_hyeto_max))
-    SV.prepare(reqs)
+    SV.prepare(reqs, SV.TopoBank(3, 2048, 4) if args.serve_side_max > 512 else None)
     srv = SV.Server(precision=MIXED, hbm_limit=150 * 10 ** 9, max_classes=16, chunk_steps=16)
     rep = srv.serve(reqs, time_limit=args.serve_duration + args.serve_drain)
     d = rep.summary()
@@ -315,6 +322,8 @@ def main():
     ap.add_argument("--serve-drain", type=float, default=50.0)
     ap.add_argument("--serve-side-max", type=int, default=512)
     ap.add_argument("--serve-hyeto-max", type=int, default=3)
+    ap.add_argument("--serve-full", action="store_true",
+                    help="the full request stream (sides to 2048, 1-10 hyetograph steps, 60 s + 60 s drain)")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

@@ -77,15 +77,40 @@ def poisson_stream(rate: float = 50.0, duration: float = 60.0, seed: int = 3, si
     return reqs
 
 
-def make_case(r: Request) -> W.Case:
+class TopoBank:
+    """A few large seeded diamond-square fields (Hurst 0.8) from which fractal
+    requests crop their topography at a seeded offset: O(cells) per request
+    instead of a diamond-square per request, for streams too fast to generate
+    inputs one by one."""
+
+    def __init__(self, seed: int = 3, side: int = 2048, fields: int = 4):
+        self.side = side
+        n = max(1, math.ceil(math.log2(side - 1 if side > 2 else 2)))
+        self.fields = [W.diamond_square(n, 0.8, seed * 1000 + k)[:side, :side] for k in range(fields)]
+
+    def crop(self, side: int, rng) -> np.ndarray:
+        f = self.fields[int(rng.integers(0, len(self.fields)))]
+        i0 = int(rng.integers(0, self.side - side + 1))
+        j0 = int(rng.integers(0, self.side - side + 1))
+        return f[i0:i0 + side, j0:j0 + side]
+
+
+def make_case(r: Request, bank: Optional[TopoBank] = None) -> W.Case:
     """The request's inputs: topography, size classes (diameters log-spaced
-    2 um..2 mm, Dirichlet(2) fractions) and Ks, from its own seed."""
+    2 um..2 mm, Dirichlet(2) fractions) and Ks, from its own seed.  Fractal
+    relief grows with the catchment (1 m + 40 m x side/2048) on a 3 % tilt;
+    with a bank the fractal field is a crop of one of its fields."""
     rng = np.random.default_rng(r.seed)
     side, dx = r.side, float(r.params["dx"])
     if r.kind == "hillslope":
         slope = rng.uniform(0.05, 0.15)
         x = (np.arange(1, side + 1) - 1) * dx
         topo = slope * x[:, None] + rng.normal(0.0, 0.005, size=(side, side))
+    elif bank is not None and side <= bank.side:
+        z = bank.crop(side, rng)
+        relief = 40.0 * side / 2048.0 + 1.0
+        z = (z - z.min()) / max(z.max() - z.min(), 1e-300) * relief
+        topo = z + 0.03 * ((np.arange(1, side + 1) - 1) * dx)[:, None]
     else:
         topo = W.fractal_topo(side, side, dx, 0.8, 40.0 * side / 2048.0 + 1.0, 0.03, r.seed % (2 ** 31))
     S = r.sclass
@@ -94,12 +119,12 @@ def make_case(r: Request) -> W.Case:
     return W.Case(f"req{r.rid}", dict(r.params), topo, np.asarray(r.rain, dtype=np.float64), ds, pf)
 
 
-def prepare(reqs: Sequence[Request]) -> None:
+def prepare(reqs: Sequence[Request], bank: Optional[TopoBank] = None) -> None:
     """Materialise every request's inputs on the host (the client side; done
     before the stream starts so that input generation is not timed)."""
     for r in reqs:
         if r.case is None:
-            r.case = make_case(r)
+            r.case = make_case(r, bank)
 
 
 @dataclass
@@ -135,6 +160,8 @@ class Report:
     peak_hbm_bytes: int
     hbm_limit: int
     results: List[Result]
+    offered_cell_s: float = 0.0     # sum over arrived requests of cells x event length (simulated s)
+    served_cell_s: float = 0.0      # sum of cells x simulated time reached by the end
     host_s: Dict[str, float] = field(default_factory=dict)   # wall time per loop phase
 
     @property
@@ -148,7 +175,9 @@ class Report:
                 "pool_steps": self.pool_steps, "cell_steps_per_s": self.cell_steps_per_s,
                 "p50_s": self.p50_s, "p99_s": self.p99_s, "mean_s": self.mean_s,
                 "max_resident": self.max_resident, "peak_hbm_bytes": self.peak_hbm_bytes,
-                "hbm_limit": self.hbm_limit, "host_s": self.host_s}
+                "hbm_limit": self.hbm_limit, "host_s": self.host_s,
+                "offered_cell_seconds": self.offered_cell_s, "served_cell_seconds": self.served_cell_s,
+                "served_over_offered": (self.served_cell_s / self.offered_cell_s) if self.offered_cell_s else None}
 
 
 def percentile(xs: Sequence[float], q: float) -> Optional[float]:
@@ -195,6 +224,7 @@ class Server:
     def _loop(self, pool, reqs, time_limit, on_result) -> Report:
         t0 = self.clock()
         nxt = 0
+        reqs_by_id = {r.rid: r for r in reqs}
         queue: List[Request] = []
         live = {}            # rid -> (request, scenario, admitted time)
         results: List[Result] = []
@@ -266,10 +296,17 @@ class Server:
                 if on_result is not None:
                     on_result(res)
         wall = self.clock() - t0
+        # offered vs served simulated work: finished requests count fully,
+        # resident ones up to the time they reached, queued ones not at all
+        offered = sum(r.cells * float(r.params["tend"]) for r in reqs[:nxt])
+        served = sum(x.cells * float(reqs_by_id[x.rid].params["tend"]) for x in results)
+        for rid, (r, sc, adm) in live.items():
+            served += r.cells * float(sc.progress().t)
         lat = [x.latency for x in results]
         return Report(submitted=len(reqs), completed=len(results),
                       incomplete=len(reqs) - len(results) - len(rejected), rejected=rejected,
                       wall_s=wall, device_ms=device_ms, cell_steps=cell_steps, pool_steps=pool_steps,
                       p50_s=percentile(lat, 50), p99_s=percentile(lat, 99),
                       mean_s=(sum(lat) / len(lat)) if lat else None, max_resident=max_res,
-                      peak_hbm_bytes=peak_hbm, hbm_limit=hbm_limit, results=results, host_s=host)
+                      peak_hbm_bytes=peak_hbm, hbm_limit=hbm_limit, results=results, host_s=host,
+                      offered_cell_s=offered, served_cell_s=served)

@@ -58,8 +58,8 @@ class FakeClock:
 
 
 class _Prog:
-    def __init__(self, steps, done):
-        self.steps, self.done, self.status = steps, done, 0
+    def __init__(self, steps, done, t=0.0):
+        self.steps, self.done, self.status, self.t = steps, done, 0, t
 
 
 class _Stats:
@@ -72,7 +72,8 @@ class FakeScenario:
         self.pool, self.id, self.case, self.need, self.steps = pool, sid, case, need, 0
 
     def progress(self):
-        return _Prog(self.steps, self.steps >= self.need)
+        # one pool step advances the fake event by one simulated second
+        return _Prog(self.steps, self.steps >= self.need, float(min(self.steps, self.need)))
 
     def fields(self, names):
         return {n: np.full((self.case.nx, self.case.ny), float(self.id)) for n in names}
@@ -156,6 +157,38 @@ def test_server_admits_in_order_overlaps_and_reports():
     assert rep.p50_s == SV.percentile(lat, 50) and rep.p99_s == SV.percentile(lat, 99)
     assert rep.p99_s >= rep.p50_s > 0
     assert rep.cell_steps == sum(r.cells * r.steps for r in rep.results)
+    offered = sum(r.cells * r.params["tend"] for r in reqs)
+    assert rep.offered_cell_s == pytest.approx(offered) and rep.served_cell_s == pytest.approx(offered)
+
+
+def test_server_reports_served_fraction_when_cut_off():
+    """A stream that is stopped early: finished requests count fully, resident
+    ones up to the time they reached, queued ones not at all."""
+    reqs = SV.poisson_stream(rate=20.0, duration=5.0, seed=11, side_min=16, side_max=128, step_len=(10, 30),
+                             hyeto_steps=(1, 3))
+    SV.prepare(reqs)
+    clk = FakeClock()
+    box = {}
+
+    def factory():
+        box["pool"] = FakePool(clk, 128 * 128 * 100 * 3)
+        return box["pool"]
+
+    rep = SV.Server(pool_factory=factory, chunk_steps=4, clock=clk, sleep=clk.sleep).serve(reqs, time_limit=2.0)
+    assert rep.incomplete > 0
+    s = rep.summary()
+    assert 0 < s["served_over_offered"] < 1
+    arrived = [r for r in reqs if r.arrival <= rep.wall_s]
+    assert rep.offered_cell_s <= sum(r.cells * r.params["tend"] for r in arrived) + 1e-9
+
+
+def test_topo_bank_crops_are_seeded():
+    bank = SV.TopoBank(seed=5, side=64, fields=2)
+    reqs = SV.poisson_stream(rate=20.0, duration=1.0, seed=13, side_min=8, side_max=64)
+    a = [SV.make_case(r, bank).topo for r in reqs]
+    b = [SV.make_case(r, bank).topo for r in reqs]
+    for x, y, r in zip(a, b, reqs):
+        assert x.shape == (r.side, r.side) and np.array_equal(x, y) and np.all(np.isfinite(x))
 
 
 def test_server_rejects_what_can_never_fit_and_waits_for_memory():
