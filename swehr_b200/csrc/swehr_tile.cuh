@@ -67,11 +67,12 @@ struct PolicyF64 {
 struct PolicyF32 {
     typedef float R;
     static constexpr int kMinBlocks = 3;
-    static __device__ __forceinline__ R sqrtp(R x)
-    {
-        const float r = __fsqrt_rn(x);
-        return (r == 0.f) ? 0.f : r;
-    }
+    /* sqrt on the SFU, x * rsqrt(x) (~3 ulp): the mixed form's ~25 square
+     * roots per cell (wave speeds, gravity, settling, friction) cost a third
+     * of the IEEE sequence; +0 for x <= 0 (the reference's pow(x, 0.5) of a
+     * zero).  The product is rounded on its own (never fused into a later
+     * add), so the single-domain and batched kernels compute the same value. */
+    static __device__ __forceinline__ R sqrtp(R x) { return x > 0.f ? __fmul_rn(x, rsqrtf(x)) : 0.f; }
     /* x^y for x > 0 as x^n * 2^(f log2 x), n = floor(y), f = y - n in [0,1):
      * the integer power by multiplication (|n| <= 4), the fractional one on
      * the SFU.  The SFU's log2 error is then scaled by f < 1 instead of y, so

@@ -116,13 +116,17 @@ def test_pool_mixed_alone_vs_mix():
     each = [_pool_all([c], MIXED)[0] for c in cases]
     mix = _pool_all(cases, MIXED, join_after=[0, 3, 9, 0, 20, 1])
     _check_same(mix, each, "mixed mix vs alone-in-pool")
-    # the single-domain mixed form computes the same per-cell arithmetic
-    alone = [_alone(c, MIXED) for c in cases]
-    for k, (g, r) in enumerate(zip(mix, alone)):
-        assert g[0] == r[0]
-        res = compare(g[1], r[1], ("h", "totsed", "sed"))
-        for name, (rel, same_nan, _) in res.items():
-            assert same_nan and rel <= 1e-4, (k, name, rel)
+    # and the pooled mixed form meets the mixed form's accuracy rule against
+    # FP64: within 1e-4, or 10x the drift FP32-rounded inputs alone cause
+    from swehr_b200.accuracy import quantized_case
+    for k, (g, c) in enumerate(zip(mix, cases)):
+        f64 = _alone(c, FP64)                  # all three end at t = tend (the last step is clamped);
+        fq = _alone(quantized_case(c), FP64)   # their step counts may differ by one
+        em, eq = compare(g[1], f64[1], ("h", "totsed", "sed")), compare(fq[1], f64[1], ("h", "totsed", "sed"))
+        for name in ("h", "totsed", "sed"):
+            env = eq[name][0]
+            bound = 1e-4 if env < 1e-5 else max(1e-4, 10 * env)
+            assert em[name][1] and em[name][0] <= bound, (k, name, em[name][0], env)
 
 
 def test_pool_budget_closes():
