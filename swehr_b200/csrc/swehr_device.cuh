@@ -181,15 +181,6 @@ __device__ __forceinline__ double rain_at(const DevParams &P, const double *__re
     return rain[rind - 1];
 }
 
-/* moving Gaussian storm (extension) */
-__device__ __forceinline__ double storm_at(const DevParams &P, double t, int i, int j)
-{
-    double x = ((double)i - 0.5) * P.dx - (P.storm_x0 + P.storm_vx * t);
-    double y = ((double)j - 0.5) * P.dx - (P.storm_y0 + P.storm_vy * t);
-    double r2 = (x * x + y * y) / P.storm_r2;
-    return P.storm_peak * sw_exp(-0.5 * r2);
-}
-
 /* hard-wired inflow ghost at j = ny+1, SWEHR.c:1019-1034 */
 __device__ __forceinline__ void inflow_ghost(double t, double &h, double &hv, double &sed)
 {
@@ -200,33 +191,6 @@ __device__ __forceinline__ void inflow_ghost(double t, double &h, double &hv, do
     hv = vin;
     sed = ukin / hin;
 }
-
-/* streampowererosion, SWEHR.c:412-426 */
-__device__ __forceinline__ double spe(double uh, double vh, double h, double beta, double rho, double g,
-                                      double sedconc, double sf, double minmorph, double uc)
-{
-    double q = sw_sqrt_pow(uh * uh + vh * vh);
-    double omega = rho * g * sf * q;
-    double E = 0;
-    if (omega > uc && sedconc < 0.6 && h > minmorph) E = beta * (omega - uc);
-    return E;
-}
-
-/* SED_k at the start of a step, as stored by the previous update
- * (SWEHR.c:1516-1530, 1549): U_k/h clamped at -1e-5, zero when dry. */
-__device__ __forceinline__ double sed_of(double uk, double h, double hfilm)
-{
-    if (!(h > hfilm)) return 0.0;
-    double s = uk / h;
-    return (s < -1e-5) ? 0.0 : s;
-}
-
-/* Face-neighbour state: interior or ghost (SWEHR.c:816-1035). */
-struct Nb {
-    double h, hu, hv;
-    int64_t q;       /* plane index of the source cell */
-    int inflow;      /* 1: inflow ghost (sed = sedin for every class) */
-};
 
 /* Budget accumulation in double-double (two-sum). */
 __device__ __forceinline__ void dd_add(double &hi, double &lo, double x)

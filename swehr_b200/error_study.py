@@ -21,8 +21,6 @@ import json
 import sys
 import time
 
-import numpy as np
-
 from . import workloads as W
 from .accuracy import quantized_case, rel_linf
 from .params import FP64, MIXED
