@@ -42,7 +42,7 @@ struct FormLauncher {
         if (occ < 1) occ = 1;
         return cudaSuccess;
     }
-    static size_t wave_smem() { return StagedLayout::make(0, sizeof(R), 0).total; }
+    static size_t wave_smem() { return 0; }   /* the wave pass stages nothing */
 
     template <int MAXS, bool BUDGET, bool SM>
     static void *update_fn() { return (void *)k_update_tile<PP, RS, MAXS, BUDGET, SM>; }
@@ -65,7 +65,7 @@ struct FormLauncher {
     {
         const int64_t ntiles = (int64_t)((P.nx + T_I - 1) / T_I) * ((P.ny + T_J - 1) / T_J);
         void *fu = nullptr;
-        void *fw = (void *)k_wave_tile<PP, RS>;
+        void *fw = (void *)k_wave_cells<PP, RS>;
         size_t su = 0;
         const size_t sw = wave_smem();
         int occ_u = 0, occ_w = 0, stage_m = 1;

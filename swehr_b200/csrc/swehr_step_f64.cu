@@ -4,9 +4,10 @@
  * to the CPU restatement built with the project's math.
  *
  * A step is two stream-ordered launches and needs no grid barrier:
- *   k_wave_tile   largest wave speed over every face (SWEHR.c:1092-1230's
- *                 Smax); the last block to finish computes dt and the Courant
- *                 check (SWEHR.c:1409-1413) and arms the update;
+ *   k_wave_cells  largest wave speed over every face (SWEHR.c:1092-1230's
+ *                 Smax), one cell's faces per thread straight from global
+ *                 memory; the last block to finish computes dt and the
+ *                 Courant check (SWEHR.c:1409-1413) and arms the update;
  *   k_update_tile fluxes, sources and the update of every cell (SWEHR.c:
  *                 1233-1588), reading state set n%2 and writing set (n+1)%2;
  *                 the last block sums the budget partials, advances t and the

@@ -438,48 +438,67 @@ __device__ __forceinline__ const RS *staged_h(const unsigned char *smb, const St
 }
 
 /* ------------------------------------------------------------------ wave */
-/* Largest wave speed over the faces a tile owns: i+1/2 and j+1/2 of its
- * cells plus the domain's low boundary faces 1/2 (SWEHR.c:1092-1230's Smax).
- * The whole block calls it; every thread returns its own partial max. */
+/* Largest wave speed over the faces cell (i, j) owns: i+1/2 and j+1/2, plus
+ * the domain's faces 1/2 when i == 1 or j == 1, so every face of
+ * SWEHR.c:1092-1230's Smax is taken once.  The cell's velocities, its GZ of
+ * the previous step and sqrt(GZ h) are formed once and serve as the left
+ * state of its faces; of the right cells only depth and normal velocity are
+ * needed.  Ghost cells follow the reference's boundary copies
+ * (SWEHR.c:816-1035): the source cell's state with the normal momentum
+ * negated at a wall, the hard-wired inflow at j = ny+1.  Reads global memory
+ * directly (no staging, no barrier): the pass is light, and a max does not
+ * depend on the order the faces are visited in. */
 template <class PP, class RS>
-__device__ __forceinline__ typename PP::R wave_tile(const DevParams &P, const SetV<RS> &src,
-                                                    const double *__restrict__ zp, TileCoord tc, unsigned char *smb,
-                                                    const StagedLayout &L, double t)
+__device__ __forceinline__ typename PP::R wave_cell(const DevParams &P, const SetV<RS> &src,
+                                                    const double *__restrict__ zp, int i, int j,
+                                                    typename PP::R inh, typename PP::R inhv)
 {
     typedef typename PP::R R;
     const RealC<R> &K = kc<R>(P);
-    double inh = 0, inhv = 0, insed = 0;
-    if (P.inflow) inflow_ghost(t, inh, inhv, insed);
-    const R *su = reinterpret_cast<const R *>(smb + L.u), *sv = reinterpret_cast<const R *>(smb + L.v);
-    const R *sg = reinterpret_cast<const R *>(smb + L.g), *sc = reinterpret_cast<const R *>(smb + L.c);
-    stage_load<RS, 0>(P, src, zp, nullptr, nullptr, tc, smb, L);
-    __pipeline_wait_prior(0);
-    __syncthreads();
-    stage_derive<PP, RS, 0>(P, tc, smb, L, (R)inh, (R)inhv, (R)insed);
-    __syncthreads();
-    const RS *sh = staged_h<RS>(smb, L);
-    R smax = 0;
-    for (int f = threadIdx.x; f < N_FX + N_FY; f += TILE_THREADS) {
-        if (f < N_FX) {
-            const int fi = f / T_J, fj = f - fi * T_J;
-            const int gi = tc.i0 - 1 + fi, gj = tc.j0 + fj;
-            if (gj > P.ny || gi > P.nx || (fi == 0 && gi != 0)) continue;
-            const int Lh = fi * H_J + fj + 1, Rh = Lh + H_J;
-            const R s = hll_speed<PP>((R)sh[fi * R_J + fj + 2], (R)sh[(fi + 1) * R_J + fj + 2], su[Lh], su[Rh],
-                                      sg[Lh], sc[Lh], K.hfilm);
-            smax = (s > smax) ? s : smax;
-        } else {
-            const int f2 = f - N_FX;
-            const int fi = f2 / (T_J + 1), fj = f2 - fi * (T_J + 1);
-            const int gi = tc.i0 + fi, gj = tc.j0 - 1 + fj;
-            if (gi > P.nx || gj > P.ny || (fj == 0 && gj != 0)) continue;
-            const int Lh = (fi + 1) * H_J + fj, Rh = Lh + 1;
-            const R s = hll_speed<PP>((R)sh[(fi + 1) * R_J + fj + 1], (R)sh[(fi + 1) * R_J + fj + 2], sv[Lh],
-                                      sv[Rh], sg[Lh], sc[Lh], K.hfilm);
-            smax = (s > smax) ? s : smax;
-        }
+    const int64_t q = cidx(P, i, j);
+    const R h = (R)src.h[q], hu = (R)src.hu[q], hv = (R)src.hv[q];
+    R u = 0, v = 0;
+    if (h > K.hfilm) {
+        u = PP::div(hu, h);
+        v = PP::div(hv, h);
     }
-    __syncthreads();
+    const R sx = (R)slope_x(P, zp, i, j), sy = (R)slope_y(P, zp, i, j);
+    const R g = PP::div(K.g, PP::sqrtp(sx * sx + sy * sy + 1));
+    const R c = PP::sqrtp(g * h);
+    R smax = 0, s;
+    /* x face i+1/2 */
+    if (i < P.nx) {
+        const int64_t qr = q + P.pitch;
+        const R hr = (R)src.h[qr];
+        const R ur = hr > K.hfilm ? PP::div((R)src.hu[qr], hr) : R(0);
+        s = hll_speed<PP>(h, hr, u, ur, g, c, K.hfilm);
+    } else {
+        s = hll_speed<PP>(h, h, u, P.bndry[2] == 1 ? -u : u, g, c, K.hfilm);
+    }
+    smax = (s > smax) ? s : smax;
+    /* y face j+1/2 */
+    if (j < P.ny) {
+        const int64_t qr = q + 1;
+        const R hr = (R)src.h[qr];
+        const R vr = hr > K.hfilm ? PP::div((R)src.hv[qr], hr) : R(0);
+        s = hll_speed<PP>(h, hr, v, vr, g, c, K.hfilm);
+    } else if (P.inflow) {
+        const R hr = (R)(RS)inh;             /* the ghost's depth as the tile pass staged it */
+        const R vr = inh > K.hfilm ? PP::div(inhv, inh) : R(0);
+        s = hll_speed<PP>(h, hr, v, vr, g, c, K.hfilm);
+    } else {
+        s = hll_speed<PP>(h, h, v, P.bndry[3] == 1 ? -v : v, g, c, K.hfilm);
+    }
+    smax = (s > smax) ? s : smax;
+    /* the domain's faces 1/2: ghost on the left, this cell on the right */
+    if (i == 1) {
+        s = hll_speed<PP>(h, h, P.bndry[0] == 1 ? -u : u, u, g, c, K.hfilm);
+        smax = (s > smax) ? s : smax;
+    }
+    if (j == 1) {
+        s = hll_speed<PP>(h, h, P.bndry[1] == 1 ? -v : v, v, g, c, K.hfilm);
+        smax = (s > smax) ? s : smax;
+    }
     return smax;
 }
 
@@ -515,23 +534,31 @@ __device__ __forceinline__ void wave_finalize(const DevParams &P, Ctl *ctl)
 }
 
 template <class PP, class RS>
-__global__ void __launch_bounds__(TILE_THREADS) k_wave_tile(const DevParams P, const BufsT<RS> B, Ctl *ctl)
+__global__ void __launch_bounds__(TILE_THREADS) k_wave_cells(const DevParams P, const BufsT<RS> B, Ctl *ctl)
 {
     typedef typename PP::R R;
     if (!ctl->active) return;
-    extern __shared__ __align__(16) unsigned char smb[];
     __shared__ double red8[TILE_THREADS / 32];
     __shared__ bool last;
-    const StagedLayout L = StagedLayout::make(0, sizeof(R), 0);
     const int64_t n = ctl->step;
     const double t = ctl->t;
     const SetV<RS> src = B.set[n & 1];
     const double *zp = B.z[(n + 2) % 3];
-    const int64_t ntiles = (int64_t)((P.nx + T_I - 1) / T_I) * ((P.ny + T_J - 1) / T_J);
+    double inh = 0, inhv = 0, insed = 0;
+    if (P.inflow) inflow_ghost(t, inh, inhv, insed);
+    /* cells in i-major order, j contiguous; (i, j) advanced by the stride */
+    const int64_t total = (int64_t)P.nx * P.ny;
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    const int64_t c0 = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const int si = (int)(stride / P.ny), sj = (int)(stride - (int64_t)si * P.ny);
+    int i = (int)(c0 / P.ny) + 1, j = (int)(c0 - (int64_t)(i - 1) * P.ny) + 1;
     R smax = 0;
-    for (int64_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
-        const R s = wave_tile<PP, RS>(P, src, zp, tile_coord(P, tile), smb, L, t);
+    for (int64_t c = c0; c < total; c += stride) {
+        const R s = wave_cell<PP, RS>(P, src, zp, i, j, (R)inh, (R)inhv);
         smax = (s > smax) ? s : smax;
+        i += si;
+        j += sj;
+        if (j > P.ny) { j -= P.ny; i++; }
     }
     const double m = block_max((double)smax, red8);
     if (threadIdx.x == 0) {
@@ -1184,17 +1211,16 @@ template <class PP, class RS>
 __global__ void __launch_bounds__(TILE_THREADS) k_wave_batch(const BatchHdr<RS> *__restrict__ hdr)
 {
     typedef typename PP::R R;
-    extern __shared__ __align__(16) unsigned char smb[];
     __shared__ double red8[TILE_THREADS / 32];
     __shared__ __align__(16) ScenDesc<RS> sd;
     __shared__ StepSnap snap;
-    const StagedLayout L = StagedLayout::make(0, sizeof(R), 0);
     const ScenDesc<RS> *tab = hdr->tab;
     const int32_t *map = hdr->tile_scen;
     const int64_t total = hdr->total_tiles;
     int cur = -1;
     unsigned run = 0;                    /* tiles of `cur` done and not yet counted */
     R smax = 0;
+    double snap_inh = 0, snap_inhv = 0;  /* the scenario's inflow ghost at this step */
     auto flush = [&]() {
         const double m = block_max((double)smax, red8);
         if (threadIdx.x == 0) {
@@ -1218,12 +1244,18 @@ __global__ void __launch_bounds__(TILE_THREADS) k_wave_batch(const BatchHdr<RS> 
             if (run) flush();
             load_desc(tab, sid, sd, snap, false);
             cur = sid;
+            double insed = 0;
+            snap_inh = snap_inhv = 0;
+            if (sd.P.inflow) inflow_ghost(snap.t, snap_inh, snap_inhv, insed);
         }
         if (!snap.go) continue;
         const int64_t n = snap.n;
-        const R s = wave_tile<PP, RS>(sd.P, sd.B.set[n & 1], sd.B.z[(n + 2) % 3], tile_coord(sd.P, g - sd.tile0),
-                                      smb, L, snap.t);
-        smax = (s > smax) ? s : smax;
+        const TileCoord tc = tile_coord(sd.P, g - sd.tile0);
+        const int i = tc.i0 + (int)threadIdx.x / T_J, j = tc.j0 + (int)threadIdx.x % T_J;
+        if (i <= sd.P.nx && j <= sd.P.ny) {
+            const R s = wave_cell<PP, RS>(sd.P, sd.B.set[n & 1], sd.B.z[(n + 2) % 3], i, j, (R)snap_inh, (R)snap_inhv);
+            smax = (s > smax) ? s : smax;
+        }
         run++;
     }
     if (run) flush();
