@@ -249,18 +249,24 @@ def ensemble_leg(args, ranks):
             envm[n] = max(envm[n], rel_linf(q[n], b[n]))
     err = {n: ranks.max(v) for n, v in err.items()}
     envm = {n: ranks.max(v) for n, v in envm.items()}
-    # the same scenarios one at a time through the single-domain path (FP64)
-    t_dev, cs = 0.0, 0
+    # the same scenarios one at a time through the single-domain path
     step = max(1, len(all_cases) // 32)
-    for k in mine:
-        if k % step:
-            continue
-        with Simulation(all_cases[k]) as sim:
-            sim.advance(max_steps=3)
-            pr = sim.advance(max_steps=args.ens_solo_steps)
-            t_dev += pr.device_ms
-            cs += all_cases[k].cells() * pr.steps_this_call
-    solo = ranks.sum(cs) / (ranks.sum(t_dev) / 1e3) if ranks.sum(t_dev) > 0 else None
+
+    def solo_rate(prec):
+        t_dev, cs = 0.0, 0
+        for k in mine:
+            if k % step:
+                continue
+            with Simulation(all_cases[k], precision=prec) as sim:
+                sim.advance(max_steps=3)
+                pr = sim.advance(max_steps=args.ens_solo_steps)
+                t_dev += pr.device_ms
+                cs += all_cases[k].cells() * pr.steps_this_call
+        tot = ranks.sum(t_dev)
+        return ranks.sum(cs) / (tot / 1e3) if tot > 0 else None
+
+    solo = solo_rate(FP64)
+    solo_mixed = solo_rate(MIXED)
     return {"workload": f"{len(all_cases)} scenarios, sides log-uniform 64..1024 (seed 2), {cells} cells, 7 classes",
             "scenarios": len(all_cases), "cells": cells, "steps_per_scenario": cap,
             "placement": f"split over {ranks.world} GPU(s) by cells, no exchange"
@@ -268,6 +274,8 @@ def ensemble_leg(args, ranks):
             "batched_mixed": out["mixed"], "batched_fp64": out["fp64"],
             "solo_fp64": {"value": solo, "unit": "cell-steps/s per GPU",
                           "sample": f"every {step}th scenario alone, {args.ens_solo_steps} steps each"},
+            "solo_mixed": {"value": solo_mixed, "unit": "cell-steps/s per GPU",
+                           "sample": f"every {step}th scenario alone, {args.ens_solo_steps} steps each"},
             "mixed_over_batched_fp64": out["mixed"]["value"] / out["fp64"]["value"],
             "mixed_over_solo_fp64": (out["mixed"]["value"] / ranks.world / solo) if solo else None,
             "error_vs_fp64": {"scenarios": [int(k) for k in range(0, len(all_cases), every)][:8], "rel_linf": err,
