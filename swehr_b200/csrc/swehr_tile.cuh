@@ -50,6 +50,10 @@ namespace swehr {
 struct PolicyF64 {
     typedef double R;
     static constexpr int kMinBlocks = 2;      /* CTAs per SM the update kernel is register-budgeted for */
+    /* the class loop of the cell update kept rolled: its unrolled body (eight
+     * inline exp and division sequences) costs more in instruction fetch
+     * than unrolling gains (measured: update -4 % rolled) */
+    static constexpr bool kRollClasses = true;
     static __device__ __forceinline__ R sqrtp(R x) { return sw_sqrt_pow(x); }
     static __device__ __forceinline__ R pow(R x, R y) { return sw_pow(x, y); }
     static __device__ __forceinline__ R exp(R x) { return sw_exp(x); }
@@ -67,6 +71,7 @@ struct PolicyF64 {
 struct PolicyF32 {
     typedef float R;
     static constexpr int kMinBlocks = 3;
+    static constexpr bool kRollClasses = false;   /* unrolled is 2 % faster here */
     /* sqrt on the SFU, x * rsqrt(x) (~3 ulp): the mixed form's ~25 square
      * roots per cell (wave speeds, gravity, settling, friction) cost a third
      * of the IEEE sequence; +0 for x <= 0 (the reference's pow(x, 0.5) of a
@@ -780,23 +785,24 @@ __device__ __forceinline__ void tile_cell(const DevParams &P, const SetV<RS> &sr
     const double vinf = vinf0 + infl;
     h = (R)(hd - infl);
 
-    /* classes (SWEHR.c:1454-1511) */
+    /* classes (SWEHR.c:1454-1511).  Class k's U_k after the face fluxes is
+     * formed at the top of its iteration, and its final value goes back to
+     * this cell's own slot of the staged U_k plane (no other thread reads
+     * that slot once the faces are solved): no per-class array stays live in
+     * registers across the loop. */
+    static_assert(sizeof(R) == sizeof(RS), "the staged U_k slot holds a U_k value");
     const R *SED = reinterpret_cast<const R *>(smb + L.sed);
-    R Uk[MAXS];
-#pragma unroll
-    for (int k = 0; k < MAXS; k++) {
-        if (k >= S) break;
-        const R *sk = SED + k * N_H;
-        Uk[k] = (R)halo[((HP_U + k) * HALO_ROWS) * R_J + so] - dtdx * (fxr0 * sk[uxr] - fxl0 * sk[uxl])
-                - dtdx * (fyr0 * sk[uyr] - fyl0 * sk[uyl]);
-    }
+    RS *Uslot = reinterpret_cast<RS *>(const_cast<unsigned char *>(smb) + L.halo) + (HP_U * HALO_ROWS) * R_J + so;
     double z = zcs[(ti + 1) * R_J + (tj + 2)];
     double totm = 0, dep = 0;
     R chtemp = 0, bulk = 0;
-#pragma unroll
+#pragma unroll ((BUDGET || !PP::kRollClasses) ? MAXS : 1)
     for (int k = 0; k < MAXS; k++) {
         if (k >= S) break;
         const int64_t qm = k * pl + q;
+        const R *sk = SED + k * N_H;
+        const RS u_in = Uslot[k * (HALO_ROWS * R_J)];
+        const R uflux = (R)u_in - dtdx * (fxr0 * sk[uxr] - fxl0 * sk[uxl]) - dtdx * (fyr0 * sk[uyr] - fyl0 * sk[uyl]);
         const double Mk0 = L.stage_m ? celld[(CD_M + k) * T_I * T_J + cs] : __ldg(src.M + qm);
         const R Mk0r = (R)Mk0;
         R E1 = 0, E2 = 0, E3 = 0, E4 = 0;
@@ -815,7 +821,7 @@ __device__ __forceinline__ void tile_cell(const DevParams &P, const SetV<RS> &sr
         if (debris) { E1 = E2 = E3 = E4 = 0; VF = 0; }
 
         double Mk = Mk0;
-        R u = Uk[k];
+        R u = uflux;
         double det_k = 0;         /* original soil detached into U_k + M_k this step (budget) */
         if (h < K.hfx10) {
             Mk += (double)(dtr * E1 + u);
@@ -844,15 +850,14 @@ __device__ __forceinline__ void tile_cell(const DevParams &P, const SetV<RS> &sr
         bulk += dh;
         totm += Mk;
         dep += PP::dep_of(Mk, P);
-        Uk[k] = u;
+        Uslot[k * (HALO_ROWS * R_J)] = (RS)u;
         dst.M[qm] = Mk;
         if (BUDGET) {
             /* U_k + M_k changes only by the face fluxes and detachment; what
              * the arithmetic and storage add on top is accounted as rounding */
-            const R *sk = SED + k * N_H;
             const double div = ((double)(fxr0 * sk[uxr]) - (double)(fxl0 * sk[uxl]))
                                + ((double)(fyr0 * sk[uyr]) - (double)(fyl0 * sk[uyl]));
-            const double change = ((double)(RS)u - (double)halo[((HP_U + k) * HALO_ROWS) * R_J + so]) + (Mk - Mk0);
+            const double change = ((double)(RS)u - (double)u_in) + (Mk - Mk0);
             acc.det[k] += det_k;
             acc.sround[k] += change - (-(dt * P.oneoverdx) * div + det_k);
         }
@@ -864,8 +869,9 @@ __device__ __forceinline__ void tile_cell(const DevParams &P, const SetV<RS> &sr
 #pragma unroll
         for (int k = 0; k < MAXS; k++) {
             if (k >= S) break;
-            totsed += PP::div(PP::div(Uk[k], h), rhos);
-            dst.U[k * pl + q] = (RS)Uk[k];
+            const R uk = (R)Uslot[k * (HALO_ROWS * R_J)];
+            totsed += PP::div(PP::div(uk, h), rhos);
+            dst.U[k * pl + q] = (RS)uk;
         }
     } else {
         clamp = hfilm - h;
@@ -876,8 +882,9 @@ __device__ __forceinline__ void tile_cell(const DevParams &P, const SetV<RS> &sr
         for (int k = 0; k < MAXS; k++) {
             if (k >= S) break;
             const int64_t qm = k * pl + q;
-            z = z + P.invporo * (double)Uk[k];
-            dst.M[qm] = dst.M[qm] + (double)Uk[k];
+            const R uk = (R)Uslot[k * (HALO_ROWS * R_J)];
+            z = z + P.invporo * (double)uk;
+            dst.M[qm] = dst.M[qm] + (double)uk;
             dst.U[qm] = (RS)0;
         }
     }
