@@ -54,6 +54,9 @@ struct PolicyF64 {
      * inline exp and division sequences) costs more in instruction fetch
      * than unrolling gains (measured: update -4 % rolled) */
     static constexpr bool kRollClasses = true;
+    /* wave pass register-budgeted for 5 CTAs per SM (48 registers): more
+     * loads in flight outweigh a few spills (measured: pass -6 %) */
+    static constexpr int kWaveMinBlocks = 5;
     static __device__ __forceinline__ R sqrtp(R x) { return sw_sqrt_pow(x); }
     static __device__ __forceinline__ R pow(R x, R y) { return sw_pow(x, y); }
     static __device__ __forceinline__ R exp(R x) { return sw_exp(x); }
@@ -72,6 +75,7 @@ struct PolicyF32 {
     typedef float R;
     static constexpr int kMinBlocks = 3;
     static constexpr bool kRollClasses = false;   /* unrolled is 2 % faster here */
+    static constexpr int kWaveMinBlocks = 8;      /* full occupancy, 32 registers, no spills */
     /* sqrt on the SFU, x * rsqrt(x) (~3 ulp): the mixed form's ~25 square
      * roots per cell (wave speeds, gravity, settling, friction) cost a third
      * of the IEEE sequence; +0 for x <= 0 (the reference's pow(x, 0.5) of a
@@ -422,7 +426,7 @@ __device__ __forceinline__ void stage_derive(const DevParams &P, TileCoord tc, u
             sc[idx] = PP::sqrtp(g * h);
         }
         if (WHAT == 1) {
-            for (int k = 0; k < P.S; k++) {
+            auto sed_k = [&](int k) {
                 R s = 0;
                 if (inflow) s = insed;
                 else if (h > K.hfilm) {
@@ -430,6 +434,12 @@ __device__ __forceinline__ void stage_derive(const DevParams &P, TileCoord tc, u
                     if (s < R(-1e-5)) s = 0;
                 }
                 ssed[k * N_H + idx] = s;
+            };
+            if (PP::kRollClasses) {          /* one division sequence in the code, not four */
+#pragma unroll 1
+                for (int k = 0; k < P.S; k++) sed_k(k);
+            } else {
+                for (int k = 0; k < P.S; k++) sed_k(k);
             }
         }
     }
@@ -539,7 +549,7 @@ __device__ __forceinline__ void wave_finalize(const DevParams &P, Ctl *ctl)
 }
 
 template <class PP, class RS>
-__global__ void __launch_bounds__(TILE_THREADS) k_wave_cells(const DevParams P, const BufsT<RS> B, Ctl *ctl)
+__global__ void __launch_bounds__(TILE_THREADS, PP::kWaveMinBlocks) k_wave_cells(const DevParams P, const BufsT<RS> B, Ctl *ctl)
 {
     typedef typename PP::R R;
     if (!ctl->active) return;
