@@ -43,6 +43,10 @@ struct BatchHdr {
     int32_t nscen, pad;
     int64_t total_tiles;
     const int32_t *tile_scen;        /* scenario of each tile of the list */
+    /* tile counters the blocks take work from: [0] wave pass, [1] update
+     * pass.  Each pass resets the other's counter (the other pass is not
+     * running then, by stream order), so both are 0 when their pass starts. */
+    unsigned long long *grab;
 };
 
 /* the batched kernels of one form (both take one argument: the header) */

@@ -98,6 +98,10 @@ struct swehr_pool {
     } while (0)
 
 static const size_t kBlockGrain = (size_t)2 << 20;
+/* the header allocation (256 bytes) holds the batch header at 0 and the two
+ * tile counters of the batched passes here */
+#define HDR_GRAB_OFFSET 128
+static_assert(sizeof(BatchHdr<double>) <= HDR_GRAB_OFFSET, "header overlaps the tile counters");
 
 /* keep resident + cached within the HBM limit: drop the largest cached blocks */
 static void trim_cache(swehr_pool *pl, size_t incoming)
@@ -244,6 +248,7 @@ static int rebuild_table(swehr_pool *pl)
     h.pad = 0;
     h.total_tiles = tile0;
     h.tile_scen = pl->d_map;
+    h.grab = reinterpret_cast<unsigned long long *>(pl->d_hdr + HDR_GRAB_OFFSET);
     memcpy(pl->h_hdr, &h, sizeof h);
     if (k > 0) PCK(cudaMemcpyAsync(pl->d_tab, pl->h_tab, (size_t)k * pl->desc_bytes, cudaMemcpyHostToDevice, pl->stream));
     if (tile0 > 0)
@@ -401,6 +406,7 @@ int swehr_pool_create(int precision, int max_classes, int budget, size_t hbm_lim
     PCKF(cudaEventCreate(&pl->ev1));
     PCKF(cudaMalloc((void **)&pl->d_hdr, 256));
     PCKF(cudaMallocHost((void **)&pl->h_hdr, 256));
+    PCKF(cudaMemsetAsync(pl->d_hdr, 0, 256, pl->stream));   /* tile counters start at 0 */
     PCKF(cudaMalloc((void **)&pl->d_tab, (size_t)max_scenarios * pl->desc_bytes));
     PCKF(cudaMallocHost((void **)&pl->h_tab, (size_t)max_scenarios * pl->desc_bytes));
     PCKF(cudaMalloc((void **)&pl->d_sum, (size_t)max_scenarios * sizeof(ScenSummary)));

@@ -1194,6 +1194,34 @@ __global__ void __launch_bounds__(TILE_THREADS, PP::kMinBlocks) k_update_tile(co
  * after every store.  Thread 0 also snapshots the scenario's step state: it
  * cannot change while this block still holds uncounted tiles of it (the
  * scenario's pass ends only once every tile is counted). */
+/* Work distribution of the batched passes: a block takes TILE_CHUNK
+ * consecutive tiles of the list at a time from a global counter, so blocks
+ * that start late or draw slow tiles take fewer (a fixed stride leaves the
+ * whole launch waiting on the slowest block), and consecutive tiles mostly
+ * share one scenario's descriptor.  The whole block calls grab_chunk; it
+ * returns false once the list is exhausted. */
+#define TILE_CHUNK 2
+struct TileChunk {
+    int64_t g0;
+    int n;
+    int sid[TILE_CHUNK];
+};
+
+__device__ __forceinline__ bool grab_chunk(unsigned long long *counter, const int32_t *__restrict__ map, int64_t total,
+                                           TileChunk &ch)
+{
+    __syncthreads();                                             /* the previous chunk is done with */
+    if (threadIdx.x == 0) {
+        const int64_t g0 = (int64_t)atomicAdd(counter, (unsigned long long)TILE_CHUNK);
+        const int64_t rest = total - g0;
+        ch.g0 = g0;
+        ch.n = rest <= 0 ? 0 : (rest < TILE_CHUNK ? (int)rest : TILE_CHUNK);
+        for (int c = 0; c < ch.n; c++) ch.sid[c] = map[g0 + c];
+    }
+    __syncthreads();
+    return ch.n > 0;
+}
+
 struct StepSnap {
     double t, dt, rain;
     int64_t n;
@@ -1253,27 +1281,32 @@ __global__ void __launch_bounds__(TILE_THREADS) k_wave_batch(const BatchHdr<RS> 
         run = 0;
         smax = 0;
     };
-    int sid_next = blockIdx.x < total ? map[blockIdx.x] : 0;
-    for (int64_t g = blockIdx.x; g < total; g += gridDim.x) {
-        const int sid = sid_next;                                /* uniform across the block */
-        if (g + gridDim.x < total) sid_next = map[g + gridDim.x];
-        if (sid != cur) {
-            if (run) flush();
-            load_desc(tab, sid, sd, snap, false);
-            cur = sid;
-            double insed = 0;
-            snap_inh = snap_inhv = 0;
-            if (sd.P.inflow) inflow_ghost(snap.t, snap_inh, snap_inhv, insed);
+    __shared__ TileChunk chunk;
+    if (blockIdx.x == 0 && threadIdx.x == 0) hdr->grab[1] = 0ull;  /* the update pass's counter, for after us */
+    for (;;) {
+        if (!grab_chunk(hdr->grab, map, total, chunk)) break;
+        for (int c = 0; c < chunk.n; c++) {
+            const int64_t g = chunk.g0 + c;
+            const int sid = chunk.sid[c];                        /* uniform across the block */
+            if (sid != cur) {
+                if (run) flush();
+                load_desc(tab, sid, sd, snap, false);
+                cur = sid;
+                double insed = 0;
+                snap_inh = snap_inhv = 0;
+                if (sd.P.inflow) inflow_ghost(snap.t, snap_inh, snap_inhv, insed);
+            }
+            if (!snap.go) continue;
+            const int64_t n = snap.n;
+            const TileCoord tc = tile_coord(sd.P, g - sd.tile0);
+            const int i = tc.i0 + (int)threadIdx.x / T_J, j = tc.j0 + (int)threadIdx.x % T_J;
+            if (i <= sd.P.nx && j <= sd.P.ny) {
+                const R s = wave_cell<PP, RS>(sd.P, sd.B.set[n & 1], sd.B.z[(n + 2) % 3], i, j, (R)snap_inh,
+                                              (R)snap_inhv);
+                smax = (s > smax) ? s : smax;
+            }
+            run++;
         }
-        if (!snap.go) continue;
-        const int64_t n = snap.n;
-        const TileCoord tc = tile_coord(sd.P, g - sd.tile0);
-        const int i = tc.i0 + (int)threadIdx.x / T_J, j = tc.j0 + (int)threadIdx.x % T_J;
-        if (i <= sd.P.nx && j <= sd.P.ny) {
-            const R s = wave_cell<PP, RS>(sd.P, sd.B.set[n & 1], sd.B.z[(n + 2) % 3], i, j, (R)snap_inh, (R)snap_inhv);
-            smax = (s > smax) ? s : smax;
-        }
-        run++;
     }
     if (run) flush();
 }
@@ -1330,20 +1363,24 @@ __global__ void __launch_bounds__(TILE_THREADS, PP::kMinBlocks) k_update_batch(c
         run = 0;
         acc_zero(acc);
     };
-    int sid_next = blockIdx.x < total ? map[blockIdx.x] : 0;
-    for (int64_t g = blockIdx.x; g < total; g += gridDim.x) {
-        const int sid = sid_next;                                /* uniform across the block */
-        if (g + gridDim.x < total) sid_next = map[g + gridDim.x];
-        if (sid != cur) {
-            if (run) flush();
-            load_desc(tab, sid, sd, snap, true);
-            cur = sid;
-            L = StagedLayout::make(sd.P.S, sizeof(R), 1, STAGE_M);
+    __shared__ TileChunk chunk;
+    if (blockIdx.x == 0 && threadIdx.x == 0) hdr->grab[0] = 0ull;  /* the wave pass's counter, for the next step */
+    for (;;) {
+        if (!grab_chunk(hdr->grab + 1, map, total, chunk)) break;
+        for (int c = 0; c < chunk.n; c++) {
+            const int64_t g = chunk.g0 + c;
+            const int sid = chunk.sid[c];                        /* uniform across the block */
+            if (sid != cur) {
+                if (run) flush();
+                load_desc(tab, sid, sd, snap, true);
+                cur = sid;
+                L = StagedLayout::make(sd.P.S, sizeof(R), 1, STAGE_M);
+            }
+            if (!snap.go) continue;
+            update_tile<PP, RS, MAXS, BUDGET>(sd.P, sd.B, snap.n, snap.t, snap.dt, snap.rain,
+                                              tile_coord(sd.P, g - sd.tile0), smb, L, acc);
+            run++;
         }
-        if (!snap.go) continue;
-        update_tile<PP, RS, MAXS, BUDGET>(sd.P, sd.B, snap.n, snap.t, snap.dt, snap.rain,
-                                          tile_coord(sd.P, g - sd.tile0), smb, L, acc);
-        run++;
     }
     if (run) flush();
 }
