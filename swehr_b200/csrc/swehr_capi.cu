@@ -591,6 +591,64 @@ static int current_step(swehr_ctx *c, int64_t *step)
     return SWEHR_OK;
 }
 
+/* |v| (d = hu, e = hv) or SED_k (d = U_k, e unused) of every cell, written
+ * contiguously (nx rows of ny) in double: the reference's derived outputs
+ * (SWEHR.c:1513-1520 SED_k = U_k/h clamped below -1e-5; vel.txt from hu/h,
+ * hv/h).  Explicit round-to-nearest operations, so the values are the ones
+ * the same expressions give on the host. */
+template <class T>
+__global__ void k_derived(const T *__restrict__ h, const T *__restrict__ d, const T *__restrict__ e, int nx, int ny,
+                          int pitch, double hfilm, int vel, double *__restrict__ out)
+{
+    const int64_t N = (int64_t)nx * ny;
+    for (int64_t q = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; q < N; q += (int64_t)gridDim.x * blockDim.x) {
+        const int i = (int)(q / ny), j = (int)(q - (int64_t)i * ny);
+        const int64_t r = (int64_t)i * pitch + j;
+        const double hh = (double)h[r];
+        double v;
+        if (vel) {
+            const double v1 = hh > hfilm ? __ddiv_rn((double)d[r], hh) : 0.0;
+            const double v2 = hh > hfilm ? __ddiv_rn((double)e[r], hh) : 0.0;
+            const double sq = __dsqrt_rn(__dadd_rn(__dmul_rn(v1, v1), __dmul_rn(v2, v2)));
+            v = (sq == 0.0) ? 0.0 : sq;
+        } else {
+            const double sd = hh > hfilm ? __ddiv_rn((double)d[r], hh) : 0.0;
+            v = (hh > hfilm && sd < -1e-5) ? 0.0 : sd;
+        }
+        out[q] = v;
+    }
+}
+
+/* A derived field computed on the device and copied back once.  Its
+ * scratch is the VINF plane (FP64 in both forms, plane >= nx*ny doubles) of
+ * the state set the next step writes: between steps that set is dead, and
+ * the next update rewrites every cell of it. */
+static int read_derived(swehr_ctx *c, int field, int k, int cur, double *dst)
+{
+    const size_t N = (size_t)c->P.nx * c->P.ny;
+    const bool vel = field == SWEHR_FIELD_VEL;
+    const PlaneRef h = field_plane(c, SWEHR_FIELD_H, 0, cur);
+    const PlaneRef d = field_plane(c, vel ? SWEHR_FIELD_HU : SWEHR_FIELD_U, k, cur);
+    const PlaneRef e = vel ? field_plane(c, SWEHR_FIELD_HV, 0, cur) : h;
+    const PlaneRef scratch = field_plane(c, SWEHR_FIELD_VINF, 0, cur ^ 1);
+    if (scratch.esize != sizeof(double) || (size_t)c->P.plane < N) return set_err(SWEHR_INVALID, "derived-field scratch plane too small");
+    double *tmp = (double *)scratch.ptr;
+    const int grid = 4 * 148, threads = 256;
+    if (h.esize == sizeof(double))
+        k_derived<double><<<grid, threads, 0, c->stream>>>((const double *)h.ptr, (const double *)d.ptr,
+                                                            (const double *)e.ptr, c->P.nx, c->P.ny, c->P.pitch,
+                                                            c->P.hfilm, vel, tmp);
+    else
+        k_derived<float><<<grid, threads, 0, c->stream>>>((const float *)h.ptr, (const float *)d.ptr,
+                                                           (const float *)e.ptr, c->P.nx, c->P.ny, c->P.pitch,
+                                                           c->P.hfilm, vel, tmp);
+    cudaError_t err = cudaGetLastError();
+    if (err == cudaSuccess) err = cudaMemcpyAsync(dst, tmp, N * sizeof(double), cudaMemcpyDeviceToHost, c->stream);
+    if (err != cudaSuccess) return set_err(SWEHR_CUDA_ERROR, std::string("derived field: ") + cudaGetErrorString(err));
+    CK(cudaStreamSynchronize(c->stream));
+    return SWEHR_OK;
+}
+
 extern "C" int swehr_read_field(swehr_ctx *c, int field, int k, double *dst)
 {
     if (!c || !dst) return set_err(SWEHR_INVALID, "NULL argument");
@@ -606,23 +664,7 @@ extern "C" int swehr_read_field(swehr_ctx *c, int field, int k, double *dst)
     if (field == SWEHR_FIELD_Z) {
         rc = download_plane(c, dst, z_plane(c, step), c->stream);
     } else if (field == SWEHR_FIELD_VEL || field == SWEHR_FIELD_SED) {
-        std::vector<double> h(N), a(N), b(N);
-        rc = download_plane(c, h.data(), field_plane(c, SWEHR_FIELD_H, 0, cur), c->stream);
-        if (!rc) rc = download_plane(c, a.data(), field_plane(c, field == SWEHR_FIELD_VEL ? SWEHR_FIELD_HU : SWEHR_FIELD_U, k, cur), c->stream);
-        if (!rc && field == SWEHR_FIELD_VEL) rc = download_plane(c, b.data(), field_plane(c, SWEHR_FIELD_HV, 0, cur), c->stream);
-        if (rc) return rc;
-        CK(cudaStreamSynchronize(c->stream));
-        for (size_t q = 0; q < N; q++) {
-            if (field == SWEHR_FIELD_VEL) {
-                double v1 = h[q] > hfilm ? a[q] / h[q] : 0, v2 = h[q] > hfilm ? b[q] / h[q] : 0;
-                double s = std::sqrt(v1 * v1 + v2 * v2);
-                dst[q] = (s == 0.0) ? 0.0 : s;
-            } else {
-                double s = h[q] > hfilm ? a[q] / h[q] : 0.0;
-                dst[q] = (h[q] > hfilm && s < -1e-5) ? 0.0 : s;
-            }
-        }
-        return SWEHR_OK;
+        return read_derived(c, field, k, cur, dst);
     } else {
         PlaneRef src = field_plane(c, field, k, cur);
         if (!src.ptr) return set_err(SWEHR_INVALID, "unknown field");

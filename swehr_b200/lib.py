@@ -126,7 +126,11 @@ class _Reader:
         d = {}
         for n in names:
             if FIELD_NAMES[n] in PER_CLASS_FIELDS:
-                d[n] = np.stack([self.field(n, k) for k in range(1, self.case.sclass + 1)])
+                # each class read straight into its slice: no stacking copy
+                out = np.empty((self.case.sclass, self.case.nx, self.case.ny))
+                for k in range(1, self.case.sclass + 1):
+                    self._check(self.L.swehr_read_field(self.ctx, FIELD_NAMES[n], k, out[k - 1].ctypes.data))
+                d[n] = out
             else:
                 d[n] = self.field(n)
         return d
