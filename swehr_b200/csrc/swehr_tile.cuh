@@ -1200,7 +1200,7 @@ __global__ void __launch_bounds__(TILE_THREADS, PP::kMinBlocks) k_update_tile(co
  * whole launch waiting on the slowest block), and consecutive tiles mostly
  * share one scenario's descriptor.  The whole block calls grab_chunk; it
  * returns false once the list is exhausted. */
-#define TILE_CHUNK 2
+#define TILE_CHUNK 4
 struct TileChunk {
     int64_t g0;
     int n;
