@@ -1194,12 +1194,15 @@ __global__ void __launch_bounds__(TILE_THREADS, PP::kMinBlocks) k_update_tile(co
  * after every store.  Thread 0 also snapshots the scenario's step state: it
  * cannot change while this block still holds uncounted tiles of it (the
  * scenario's pass ends only once every tile is counted). */
-/* Work distribution of the batched passes: a block takes TILE_CHUNK
+/* Work distribution of the batched passes: a block takes a chunk of
  * consecutive tiles of the list at a time from a global counter, so blocks
  * that start late or draw slow tiles take fewer (a fixed stride leaves the
  * whole launch waiting on the slowest block), and consecutive tiles mostly
- * share one scenario's descriptor.  The whole block calls grab_chunk; it
- * returns false once the list is exhausted. */
+ * share one scenario's descriptor.  Chunks are TILE_CHUNK tiles when every
+ * block gets at least eight of them, else single tiles, so a small pool
+ * (a serving mix of a few requests) still spreads over all blocks.  The
+ * whole block calls grab_chunk; it returns false once the list is
+ * exhausted. */
 #define TILE_CHUNK 4
 struct TileChunk {
     int64_t g0;
@@ -1212,10 +1215,11 @@ __device__ __forceinline__ bool grab_chunk(unsigned long long *counter, const in
 {
     __syncthreads();                                             /* the previous chunk is done with */
     if (threadIdx.x == 0) {
-        const int64_t g0 = (int64_t)atomicAdd(counter, (unsigned long long)TILE_CHUNK);
+        const int size = total >= (int64_t)8 * TILE_CHUNK * gridDim.x ? TILE_CHUNK : 1;
+        const int64_t g0 = (int64_t)atomicAdd(counter, (unsigned long long)size);
         const int64_t rest = total - g0;
         ch.g0 = g0;
-        ch.n = rest <= 0 ? 0 : (rest < TILE_CHUNK ? (int)rest : TILE_CHUNK);
+        ch.n = rest <= 0 ? 0 : (rest < size ? (int)rest : size);
         for (int c = 0; c < ch.n; c++) ch.sid[c] = map[g0 + c];
     }
     __syncthreads();
