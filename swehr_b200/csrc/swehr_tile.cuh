@@ -795,24 +795,40 @@ __device__ __forceinline__ void tile_cell(const DevParams &P, const SetV<RS> &sr
     const double vinf = vinf0 + infl;
     h = (R)(hd - infl);
 
-    /* classes (SWEHR.c:1454-1511).  Class k's U_k after the face fluxes is
-     * formed at the top of its iteration, and its final value goes back to
-     * this cell's own slot of the staged U_k plane (no other thread reads
-     * that slot once the faces are solved): no per-class array stays live in
-     * registers across the loop. */
+    /* classes (SWEHR.c:1454-1511).  U_k after the face fluxes, then its
+     * final value: the FP64 form (rolled class loop) forms it at the top of
+     * class k's iteration and keeps the final value in this cell's own slot
+     * of the staged U_k plane (no other thread reads that slot once the faces
+     * are solved), so no per-class array stays live in registers; the mixed
+     * form's unrolled loops keep them in registers (faster there). */
+    constexpr bool kSlot = PP::kRollClasses;
     static_assert(sizeof(R) == sizeof(RS), "the staged U_k slot holds a U_k value");
     const R *SED = reinterpret_cast<const R *>(smb + L.sed);
     RS *Uslot = reinterpret_cast<RS *>(const_cast<unsigned char *>(smb) + L.halo) + (HP_U * HALO_ROWS) * R_J + so;
+    R Ureg[kSlot ? 1 : MAXS];
+    if constexpr (!kSlot) {
+#pragma unroll
+        for (int k = 0; k < MAXS; k++) {
+            if (k >= S) break;
+            const R *sk = SED + k * N_H;
+            Ureg[k] = (R)Uslot[k * (HALO_ROWS * R_J)] - dtdx * (fxr0 * sk[uxr] - fxl0 * sk[uxl])
+                      - dtdx * (fyr0 * sk[uyr] - fyl0 * sk[uyl]);
+        }
+    }
     double z = zcs[(ti + 1) * R_J + (tj + 2)];
     double totm = 0, dep = 0;
     R chtemp = 0, bulk = 0;
-#pragma unroll ((BUDGET || !PP::kRollClasses) ? MAXS : 1)
+#pragma unroll ((BUDGET || !kSlot) ? MAXS : 1)
     for (int k = 0; k < MAXS; k++) {
         if (k >= S) break;
         const int64_t qm = k * pl + q;
         const R *sk = SED + k * N_H;
         const RS u_in = Uslot[k * (HALO_ROWS * R_J)];
-        const R uflux = (R)u_in - dtdx * (fxr0 * sk[uxr] - fxl0 * sk[uxl]) - dtdx * (fyr0 * sk[uyr] - fyl0 * sk[uyl]);
+        R uflux;
+        if constexpr (kSlot)
+            uflux = (R)u_in - dtdx * (fxr0 * sk[uxr] - fxl0 * sk[uxl]) - dtdx * (fyr0 * sk[uyr] - fyl0 * sk[uyl]);
+        else
+            uflux = Ureg[kSlot ? 0 : k];
         const double Mk0 = L.stage_m ? celld[(CD_M + k) * T_I * T_J + cs] : __ldg(src.M + qm);
         const R Mk0r = (R)Mk0;
         R E1 = 0, E2 = 0, E3 = 0, E4 = 0;
@@ -860,7 +876,10 @@ __device__ __forceinline__ void tile_cell(const DevParams &P, const SetV<RS> &sr
         bulk += dh;
         totm += Mk;
         dep += PP::dep_of(Mk, P);
-        Uslot[k * (HALO_ROWS * R_J)] = (RS)u;
+        if constexpr (kSlot)
+            Uslot[k * (HALO_ROWS * R_J)] = (RS)u;
+        else
+            Ureg[kSlot ? 0 : k] = u;
         dst.M[qm] = Mk;
         if (BUDGET) {
             /* U_k + M_k changes only by the face fluxes and detachment; what
@@ -879,7 +898,7 @@ __device__ __forceinline__ void tile_cell(const DevParams &P, const SetV<RS> &sr
 #pragma unroll
         for (int k = 0; k < MAXS; k++) {
             if (k >= S) break;
-            const R uk = (R)Uslot[k * (HALO_ROWS * R_J)];
+            const R uk = kSlot ? (R)Uslot[k * (HALO_ROWS * R_J)] : Ureg[kSlot ? 0 : k];
             totsed += PP::div(PP::div(uk, h), rhos);
             dst.U[k * pl + q] = (RS)uk;
         }
@@ -892,7 +911,7 @@ __device__ __forceinline__ void tile_cell(const DevParams &P, const SetV<RS> &sr
         for (int k = 0; k < MAXS; k++) {
             if (k >= S) break;
             const int64_t qm = k * pl + q;
-            const R uk = (R)Uslot[k * (HALO_ROWS * R_J)];
+            const R uk = kSlot ? (R)Uslot[k * (HALO_ROWS * R_J)] : Ureg[kSlot ? 0 : k];
             z = z + P.invporo * (double)uk;
             dst.M[qm] = dst.M[qm] + (double)uk;
             dst.U[qm] = (RS)0;
