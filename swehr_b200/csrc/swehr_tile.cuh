@@ -1351,7 +1351,10 @@ __global__ void __launch_bounds__(TILE_THREADS, PP::kMinBlocks) k_update_batch(c
     unsigned run = 0;
     Acc2<MAXS, BUDGET> acc;
     acc_zero(acc);
-    StagedLayout L = StagedLayout::make(1, sizeof(R), 1, STAGE_M);
+    /* the staging layout of the current scenario, uniform across the block:
+     * kept in shared memory rather than in every thread's registers */
+    __shared__ StagedLayout L;
+    if (threadIdx.x == 0) L = StagedLayout::make(1, sizeof(R), 1, STAGE_M);
     auto flush = [&]() {
         Ctl *ctl = sd.ctl;
         double *red = reinterpret_cast<double *>(smb + L.red);
@@ -1397,7 +1400,8 @@ __global__ void __launch_bounds__(TILE_THREADS, PP::kMinBlocks) k_update_batch(c
                 if (run) flush();
                 load_desc(tab, sid, sd, snap, true);
                 cur = sid;
-                L = StagedLayout::make(sd.P.S, sizeof(R), 1, STAGE_M);
+                if (threadIdx.x == 0) L = StagedLayout::make(sd.P.S, sizeof(R), 1, STAGE_M);
+                __syncthreads();
             }
             if (!snap.go) continue;
             update_tile<PP, RS, MAXS, BUDGET>(sd.P, sd.B, snap.n, snap.t, snap.dt, snap.rain,
