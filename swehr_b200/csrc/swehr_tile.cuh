@@ -1271,7 +1271,7 @@ __device__ __forceinline__ void load_desc(const ScenDesc<RS> *tab, int sid, Scen
     __syncthreads();
 }
 
-/* Batched wave pass.  A block walks the tile list with a grid stride and
+/* Batched wave pass.  A block takes chunks of the tile list (grab_chunk) and
  * keeps a run per scenario: consecutive tiles of one scenario share the
  * descriptor copy and a running max, and the scenario's ticket is advanced
  * by the run's tile count once, when the block moves on (or finishes). */
