@@ -10,12 +10,15 @@
  */
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <chrono>
 #include <cmath>
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <mutex>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "../../include/swehr.h"
@@ -227,9 +230,89 @@ static int upload_plane(swehr_ctx *c, PlaneRef d, const double *host, cudaStream
     return SWEHR_OK;
 }
 
+/* Rows of a device array (nrows x ncols elements of esize bytes, spitch
+ * bytes apart) into contiguous host doubles.  Planes of 32 MB and more go
+ * through two pinned 16 MB buffers, the device copy of one chunk overlapping
+ * the host copy of the one before (a pageable destination is otherwise
+ * filled at a fraction of the link's speed); smaller reads (a serving
+ * request's) and pooled contexts return 0 without copying. */
+static const size_t kStageBytes = (size_t)16 << 20;
+static const size_t kStageMin = (size_t)32 << 20;
+
+static void stage_part(double *dst, const void *src, size_t n, size_t esize)
+{
+    if (esize == sizeof(double)) {
+        memcpy(dst, src, n * sizeof(double));
+        return;
+    }
+    const float *f = (const float *)src;
+    for (size_t q = 0; q < n; q++) dst[q] = (double)f[q];
+}
+
+/* the host side of a chunk, split over a few threads: filling fresh pageable
+ * pages is bound by page faults, which proceed in parallel */
+static void stage_out(double *dst, const void *src, size_t n, size_t esize)
+{
+    const int T = 4;
+    const size_t per = (n + T - 1) / T;
+    std::thread th[T - 1];
+    for (int t = 1; t < T; t++) {
+        const size_t a = std::min(n, (size_t)t * per), b = std::min(n, a + per);
+        th[t - 1] = std::thread(stage_part, dst + a, (const char *)src + a * esize, b - a, esize);
+    }
+    stage_part(dst, src, std::min(n, per), esize);
+    for (int t = 0; t < T - 1; t++) th[t].join();
+}
+
+static int d2h_staged(swehr_ctx *c, double *host, const void *dev, size_t spitch, size_t esize, int64_t nrows,
+                      int64_t ncols, int *done)
+{
+    *done = 0;
+    const size_t row_in = (size_t)ncols * esize;
+    if (c->host || row_in * (size_t)nrows < kStageMin || row_in > kStageBytes) return SWEHR_OK;
+    /* one pinned pair per process (pinning takes ~0.1 s), used by one read at a time */
+    static std::mutex mu;
+    static void *stage = nullptr;
+    std::lock_guard<std::mutex> lock(mu);
+    if (!stage) CK(cudaHostAlloc(&stage, 2 * kStageBytes, cudaHostAllocPortable));
+    if (!c->ev_stage[0])
+        for (int e = 0; e < 2; e++) CK(cudaEventCreateWithFlags(&c->ev_stage[e], cudaEventDisableTiming));
+    c->h_stage = stage;
+    const int64_t per = (int64_t)(kStageBytes / row_in);
+    int64_t prev_r0 = -1, prev_n = 0;
+    int prev_b = 0;
+    int64_t k = 0;
+    for (int64_t r0 = 0; r0 < nrows; r0 += per, k++) {
+        const int64_t n = std::min(per, nrows - r0);
+        const int b = (int)(k & 1);
+        char *buf = (char *)c->h_stage + (size_t)b * kStageBytes;
+        CK(cudaMemcpy2DAsync(buf, row_in, (const char *)dev + (size_t)r0 * spitch, spitch, row_in, (size_t)n,
+                             cudaMemcpyDeviceToHost, c->stream));
+        CK(cudaEventRecord(c->ev_stage[b], c->stream));
+        if (prev_r0 >= 0) {
+            CK(cudaEventSynchronize(c->ev_stage[prev_b]));
+            stage_out(host + (size_t)prev_r0 * ncols, (char *)c->h_stage + (size_t)prev_b * kStageBytes,
+                      (size_t)prev_n * ncols, esize);
+        }
+        prev_r0 = r0;
+        prev_n = n;
+        prev_b = b;
+    }
+    if (prev_r0 >= 0) {
+        CK(cudaEventSynchronize(c->ev_stage[prev_b]));
+        stage_out(host + (size_t)prev_r0 * ncols, (char *)c->h_stage + (size_t)prev_b * kStageBytes,
+                  (size_t)prev_n * ncols, esize);
+    }
+    *done = 1;
+    return SWEHR_OK;
+}
+
 static int download_plane(swehr_ctx *c, double *host, PlaneRef d, cudaStream_t s)
 {
     const size_t N = (size_t)c->P.nx * c->P.ny;
+    int staged = 0;
+    int rc = d2h_staged(c, host, d.ptr, (size_t)c->P.pitch * d.esize, d.esize, c->P.nx, c->P.ny, &staged);
+    if (rc || staged) return rc;
     if (d.esize == sizeof(double)) {
         CK(cudaMemcpy2DAsync(host, (size_t)c->P.ny * sizeof(double), d.ptr, (size_t)c->P.pitch * sizeof(double),
                              (size_t)c->P.ny * sizeof(double), (size_t)c->P.nx, cudaMemcpyDeviceToHost, s));
@@ -280,6 +363,8 @@ static void destroy_ctx(swehr_ctx *c)
     if (c->ev_stop) cudaEventDestroy(c->ev_stop);
     for (int e = 0; e < 2 * TIMING_RING; e++)
         if (c->ev_k[e]) cudaEventDestroy(c->ev_k[e]);
+    for (int e = 0; e < 2; e++)
+        if (c->ev_stage[e]) cudaEventDestroy(c->ev_stage[e]);
     if (c->host) {
         if (c->mem) c->host->release(c->host->self, c->mem);
         free(c->h_ctl);
@@ -643,7 +728,13 @@ static int read_derived(swehr_ctx *c, int field, int k, int cur, double *dst)
                                                            (const float *)e.ptr, c->P.nx, c->P.ny, c->P.pitch,
                                                            c->P.hfilm, vel, tmp);
     cudaError_t err = cudaGetLastError();
-    if (err == cudaSuccess) err = cudaMemcpyAsync(dst, tmp, N * sizeof(double), cudaMemcpyDeviceToHost, c->stream);
+    if (err == cudaSuccess) {
+        int staged = 0;
+        const int rc = d2h_staged(c, dst, tmp, (size_t)c->P.ny * sizeof(double), sizeof(double), c->P.nx, c->P.ny,
+                                  &staged);
+        if (rc) return rc;
+        if (!staged) err = cudaMemcpyAsync(dst, tmp, N * sizeof(double), cudaMemcpyDeviceToHost, c->stream);
+    }
     if (err != cudaSuccess) return set_err(SWEHR_CUDA_ERROR, std::string("derived field: ") + cudaGetErrorString(err));
     CK(cudaStreamSynchronize(c->stream));
     return SWEHR_OK;

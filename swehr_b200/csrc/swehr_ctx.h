@@ -43,6 +43,8 @@ struct swehr_ctx {
     cudaGraphExec_t graph = nullptr;
     cudaEvent_t ev_start = nullptr, ev_stop = nullptr;
     cudaEvent_t ev_k[2 * TIMING_RING] = {};
+    void *h_stage = nullptr;           /* the process's two pinned download buffers (set on the first large read) */
+    cudaEvent_t ev_stage[2] = {};
     swehr::StepConfig cfg;
     int timing = 0;
     int64_t stagecap = 0;
