@@ -354,6 +354,15 @@ static void set_views(BufsT<RS> &B, char *pool, const Layout &L, int S, int has_
     B.ks = has_ks ? (const RS *)(pool + L.off_ks) : nullptr;
 }
 
+/* a plane with v in its nx x ny cells and 0 in the row padding */
+__global__ void k_fill_cells(double *__restrict__ p, int nx, int ny, int pitch, int64_t plane, double v)
+{
+    for (int64_t q = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; q < plane; q += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t i = q / pitch, j = q - i * pitch;
+        p[q] = (i < nx && j < ny) ? v : 0.0;
+    }
+}
+
 static void destroy_ctx(swehr_ctx *c)
 {
     if (!c) return;
@@ -474,21 +483,19 @@ int swehr_ctx_create(const swehr_params *p, const swehr_inputs *in, int precisio
     /* initial state (initialcondition, SWEHR.c:211-285): dry bed, VINF = vinf0, z = topo;
      * z of the previous step = z (setup slopes, SWEHR.c:721-803) */
     double *const *zpl = precision == SWEHR_MIXED ? c->B32.z : c->B64.z;
-    for (int k = 0; k < 3; k++) {
-        rc = upload_plane(c, PlaneRef{zpl[k], sizeof(double)}, in->topo, c->stream);
-        if (rc) { destroy_ctx(c); return rc; }
-    }
+    rc = upload_plane(c, PlaneRef{zpl[0], sizeof(double)}, in->topo, c->stream);
+    if (rc) { destroy_ctx(c); return rc; }
+    for (int k = 1; k < 3; k++)     /* the other two z planes from the first, on the device */
+        CKC(cudaMemcpyAsync(zpl[k], zpl[0], (size_t)c->P.plane * sizeof(double), cudaMemcpyDeviceToDevice, c->stream));
     if (in->ks) {
         void *kp = precision == SWEHR_MIXED ? (void *)c->B32.ks : (void *)c->B64.ks;
         rc = upload_plane(c, PlaneRef{kp, L.rsize}, in->ks, c->stream);
         if (rc) { destroy_ctx(c); return rc; }
     }
     {
-        std::vector<double> row((size_t)c->P.plane, 0.0);
-        for (int i = 0; i < p->nx; i++)
-            for (int j = 0; j < p->ny; j++) row[(size_t)i * c->P.pitch + j] = p->vinf0;
         double *vinf0 = precision == SWEHR_MIXED ? c->B32.set[0].vinf : c->B64.set[0].vinf;
-        CKC(cudaMemcpyAsync(vinf0, row.data(), (size_t)c->P.plane * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+        k_fill_cells<<<4 * 148, 256, 0, c->stream>>>(vinf0, p->nx, p->ny, c->P.pitch, c->P.plane, p->vinf0);
+        CKC(cudaGetLastError());
         CKC(cudaMemcpyAsync(c->d_rain, in->rain, (size_t)p->rnum * sizeof(double), cudaMemcpyHostToDevice, c->stream));
         Ctl h;
         memset(&h, 0, sizeof h);
