@@ -15,7 +15,7 @@ template <class PP, class RS>
 struct FormLauncher {
     typedef typename PP::R R;
 
-    static size_t update_smem(int S, int stage_m = 1) { return StagedLayout::make(S, sizeof(R), 1, stage_m).total; }
+    static size_t update_smem(int S, int stage_m = 1) { return StagedLayout::make(S, sizeof(R), stage_m).total; }
 
     /* The update kernel and shared memory for S classes: M_k staged unless
      * leaving it in global memory fits more blocks per SM (measured: staging

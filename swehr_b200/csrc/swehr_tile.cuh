@@ -231,28 +231,28 @@ struct StagedLayout {
     /* stage_m: staging M_k costs 2 KB of shared memory per class; the
      * launcher picks the kernel that stages it only where that costs no
      * resident blocks (a compile-time choice of each kernel) */
-    __host__ __device__ static StagedLayout make(int S, size_t rs, int what, int stage_m = 1)
+    __host__ __device__ static StagedLayout make(int S, size_t rs, int stage_m = 1)
     {
         StagedLayout L;
         size_t o = 0;
         auto take = [&](size_t bytes) { size_t at = o; o += (bytes + 15) / 16 * 16; return at; };
-        L.stage_m = what && stage_m;
-        L.nhalo = what ? 5 + S : 3;
-        L.ncellr = what ? 4 : 0;
-        L.ncelld = what ? (L.stage_m ? 1 + S : 1) : 0;
+        L.stage_m = stage_m;
+        L.nhalo = 5 + S;
+        L.ncellr = 4;
+        L.ncelld = L.stage_m ? 1 + S : 1;
         L.halo = take((size_t)L.nhalo * HALO_ROWS * R_J * rs);
         L.cell_r = take((size_t)L.ncellr * T_I * T_J * rs);
         L.cell_d = take((size_t)L.ncelld * T_I * T_J * sizeof(double));
         L.zp = take((size_t)ZP_ROWS * R_J * sizeof(double));
-        L.zc = take(what ? (size_t)ZC_ROWS * R_J * sizeof(double) : 0);
+        L.zc = take((size_t)ZC_ROWS * R_J * sizeof(double));
         L.u = take((size_t)N_H * rs);
         L.v = take((size_t)N_H * rs);
         L.g = take((size_t)N_H * rs);
         L.c = take((size_t)N_H * rs);
-        L.sed = take(what ? (size_t)S * N_H * rs : 0);
-        L.fx = take(what ? (size_t)3 * N_FX * rs : 0);
-        L.fy = take(what ? (size_t)3 * N_FY * rs : 0);
-        L.up = take(what ? (size_t)(N_FX + N_FY) : 0);
+        L.sed = take((size_t)S * N_H * rs);
+        L.fx = take((size_t)3 * N_FX * rs);
+        L.fy = take((size_t)3 * N_FY * rs);
+        L.up = take((size_t)(N_FX + N_FY));
         /* the budget reduction runs after a tile's cells are done, when the
          * face states u, v, g, c are dead: it reuses their space */
         L.red = L.u;
@@ -287,10 +287,10 @@ __device__ __forceinline__ void cp_pair(void *dst, const T *src)
     __pipeline_memcpy_async(dst, src, 2 * sizeof(T));
 }
 
-/* Issue the tile's asynchronous copies.  WHAT = 0: wave pass (h hu hv, z_prev);
- * 1: update pass (all).  Each thread owns fixed (row, pair) slots and walks
- * the planes with a pointer step, so the per-copy cost is one add. */
-template <class RS, int WHAT>
+/* Issue the tile's asynchronous copies (halo planes, z_prev and z windows,
+ * cell planes).  Each thread owns fixed (row, pair) slots and walks the
+ * planes with a pointer step, so the per-copy cost is one add. */
+template <class RS>
 __device__ __forceinline__ void stage_load(const DevParams &P, const SetV<RS> &src, const double *__restrict__ zp,
                                            const double *__restrict__ zc, const RS *__restrict__ ks, TileCoord tc,
                                            unsigned char *smb, const StagedLayout &L)
@@ -309,18 +309,16 @@ __device__ __forceinline__ void stage_load(const DevParams &P, const SetV<RS> &s
             cp_pair(d + HP_H * ps, src.h + go);
             cp_pair(d + HP_HU * ps, src.hu + go);
             cp_pair(d + HP_HV * ps, src.hv + go);
-            if (WHAT) {
-                cp_pair(d + HP_TS * ps, src.totsed + go);
-                cp_pair(d + HP_DEP * ps, src.dep + go);
-                const RS *u = src.U + go;
-                for (int k = 0; k < P.S; k++) cp_pair(d + (HP_U + k) * ps, u + (int64_t)k * pl);
-            }
+            cp_pair(d + HP_TS * ps, src.totsed + go);
+            cp_pair(d + HP_DEP * ps, src.dep + go);
+            const RS *u = src.U + go;
+            for (int k = 0; k < P.S; k++) cp_pair(d + (HP_U + k) * ps, u + (int64_t)k * pl);
         }
     }
     /* topography: z_prev 12 rows, z 10 rows, 18 pairs each */
     {
         const int slot = tid < HALO_ROWS * (R_J / 2) ? tid + (256 - HALO_ROWS * (R_J / 2)) : tid - HALO_ROWS * (R_J / 2);
-        const int nzs = (ZP_ROWS + (WHAT ? ZC_ROWS : 0)) * (R_J / 2);      /* 396 or 216 */
+        const int nzs = (ZP_ROWS + ZC_ROWS) * (R_J / 2);                   /* 396 */
         for (int s = slot; s < nzs; s += TILE_THREADS) {
             const bool isp = s < ZP_ROWS * (R_J / 2);
             const int s2 = isp ? s : s - ZP_ROWS * (R_J / 2);
@@ -331,26 +329,24 @@ __device__ __forceinline__ void stage_load(const DevParams &P, const SetV<RS> &s
             cp_pair(d, (isp ? zp : zc) + (int64_t)(gi - 1) * P.pitch + col);
         }
     }
-    if (WHAT) {
-        /* cell planes: 8 rows x 16 pairs = 128 slots; threads 128..255 */
-        if (tid >= TILE_THREADS - T_I * (T_J / 2)) {
-            const int s = tid - (TILE_THREADS - T_I * (T_J / 2));
-            const int r = s / (T_J / 2), k2 = s - r * (T_J / 2);
-            const int gi = tc.i0 + r, col = tc.j0 - 1 + 2 * k2;
-            if (gi <= P.nx && col < P.pitch) {
-                const int64_t go = (int64_t)(gi - 1) * P.pitch + col;
-                RS *cr = reinterpret_cast<RS *>(smb + L.cell_r) + r * T_J + 2 * k2;
-                double *cd = reinterpret_cast<double *>(smb + L.cell_d) + r * T_J + 2 * k2;
-                const int ps = T_I * T_J;
-                cp_pair(cr + CR_TOTM * ps, src.totm + go);
-                cp_pair(cr + CR_MAXVEL * ps, src.maxvel + go);
-                cp_pair(cr + CR_MAXDEP * ps, src.maxdep + go);
-                if (P.has_ks) cp_pair(cr + CR_KS * ps, ks + go);
-                cp_pair(cd + CD_VINF * ps, src.vinf + go);
-                if (L.stage_m) {
-                    const double *m = src.M + go;
-                    for (int k = 0; k < P.S; k++) cp_pair(cd + (CD_M + k) * ps, m + (int64_t)k * pl);
-                }
+    /* cell planes: 8 rows x 16 pairs = 128 slots; threads 128..255 */
+    if (tid >= TILE_THREADS - T_I * (T_J / 2)) {
+        const int s = tid - (TILE_THREADS - T_I * (T_J / 2));
+        const int r = s / (T_J / 2), k2 = s - r * (T_J / 2);
+        const int gi = tc.i0 + r, col = tc.j0 - 1 + 2 * k2;
+        if (gi <= P.nx && col < P.pitch) {
+            const int64_t go = (int64_t)(gi - 1) * P.pitch + col;
+            RS *cr = reinterpret_cast<RS *>(smb + L.cell_r) + r * T_J + 2 * k2;
+            double *cd = reinterpret_cast<double *>(smb + L.cell_d) + r * T_J + 2 * k2;
+            const int ps = T_I * T_J;
+            cp_pair(cr + CR_TOTM * ps, src.totm + go);
+            cp_pair(cr + CR_MAXVEL * ps, src.maxvel + go);
+            cp_pair(cr + CR_MAXDEP * ps, src.maxdep + go);
+            if (P.has_ks) cp_pair(cr + CR_KS * ps, ks + go);
+            cp_pair(cd + CD_VINF * ps, src.vinf + go);
+            if (L.stage_m) {
+                const double *m = src.M + go;
+                for (int k = 0; k < P.S; k++) cp_pair(cd + (CD_M + k) * ps, m + (int64_t)k * pl);
             }
         }
     }
@@ -376,7 +372,7 @@ __device__ __forceinline__ double sslope_y(const DevParams &P, const double *zs,
 /* Derived halo values from the staged planes: h, u = hu/h, v = hv/h (0 when
  * dry), GZ of the previous step and sqrt(GZ h) for left/lower face cells,
  * SED_k.  Ghost cells read their source cell (SWEHR.c:816-1035). */
-template <class PP, class RS, int WHAT>
+template <class PP, class RS>
 __device__ __forceinline__ void stage_derive(const DevParams &P, TileCoord tc, unsigned char *smb,
                                              const StagedLayout &L, typename PP::R inh, typename PP::R inhv,
                                              typename PP::R insed)
@@ -425,22 +421,20 @@ __device__ __forceinline__ void stage_derive(const DevParams &P, TileCoord tc, u
             sg[idx] = g;
             sc[idx] = PP::sqrtp(g * h);
         }
-        if (WHAT == 1) {
-            auto sed_k = [&](int k) {
-                R s = 0;
-                if (inflow) s = insed;
-                else if (h > K.hfilm) {
-                    s = PP::div((R)halo[((HP_U + k) * HALO_ROWS) * R_J + so], h);
-                    if (s < R(-1e-5)) s = 0;
-                }
-                ssed[k * N_H + idx] = s;
-            };
-            if (PP::kRollClasses) {          /* one division sequence in the code, not four */
-#pragma unroll 1
-                for (int k = 0; k < P.S; k++) sed_k(k);
-            } else {
-                for (int k = 0; k < P.S; k++) sed_k(k);
+        auto sed_k = [&](int k) {
+            R s = 0;
+            if (inflow) s = insed;
+            else if (h > K.hfilm) {
+                s = PP::div((R)halo[((HP_U + k) * HALO_ROWS) * R_J + so], h);
+                if (s < R(-1e-5)) s = 0;
             }
+            ssed[k * N_H + idx] = s;
+        };
+        if (PP::kRollClasses) {          /* one division sequence in the code, not four */
+#pragma unroll 1
+            for (int k = 0; k < P.S; k++) sed_k(k);
+        } else {
+            for (int k = 0; k < P.S; k++) sed_k(k);
         }
     }
 }
@@ -1045,10 +1039,10 @@ __device__ __forceinline__ void update_tile(const DevParams &P, const BufsT<RS> 
     const R *su = reinterpret_cast<const R *>(smb + L.u), *sv = reinterpret_cast<const R *>(smb + L.v);
     const R *sg = reinterpret_cast<const R *>(smb + L.g), *sc = reinterpret_cast<const R *>(smb + L.c);
     R *sfx = reinterpret_cast<R *>(smb + L.fx), *sfy = reinterpret_cast<R *>(smb + L.fy);
-    stage_load<RS, 1>(P, src, zp, zc, B.ks, tc, smb, L);
+    stage_load<RS>(P, src, zp, zc, B.ks, tc, smb, L);
     __pipeline_wait_prior(0);
     __syncthreads();
-    stage_derive<PP, RS, 1>(P, tc, smb, L, (R)inh, (R)inhv, (R)insed);
+    stage_derive<PP, RS>(P, tc, smb, L, (R)inh, (R)inhv, (R)insed);
     __syncthreads();
     const RS *sh = staged_h<RS>(smb, L);
     /* stage B: every face of the tile (SWEHR.c:1099-1230) */
@@ -1165,7 +1159,7 @@ __global__ void __launch_bounds__(TILE_THREADS, PP::kMinBlocks) k_update_tile(co
     if (!ctl->pending) return;
     extern __shared__ __align__(16) unsigned char smb[];
     __shared__ bool last;
-    const StagedLayout L = StagedLayout::make(P.S, sizeof(R), 1, STAGE_M);
+    const StagedLayout L = StagedLayout::make(P.S, sizeof(R), STAGE_M);
     const int64_t n = ctl->step;
     const double t = ctl->t, dt = ctl->dt;
     const double Rr = P.storm ? 0.0 : rain_at(P, rain, t);
@@ -1354,7 +1348,7 @@ __global__ void __launch_bounds__(TILE_THREADS, PP::kMinBlocks) k_update_batch(c
     /* the staging layout of the current scenario, uniform across the block:
      * kept in shared memory rather than in every thread's registers */
     __shared__ StagedLayout L;
-    if (threadIdx.x == 0) L = StagedLayout::make(1, sizeof(R), 1, STAGE_M);
+    if (threadIdx.x == 0) L = StagedLayout::make(1, sizeof(R), STAGE_M);
     auto flush = [&]() {
         Ctl *ctl = sd.ctl;
         double *red = reinterpret_cast<double *>(smb + L.red);
@@ -1400,7 +1394,7 @@ __global__ void __launch_bounds__(TILE_THREADS, PP::kMinBlocks) k_update_batch(c
                 if (run) flush();
                 load_desc(tab, sid, sd, snap, true);
                 cur = sid;
-                if (threadIdx.x == 0) L = StagedLayout::make(sd.P.S, sizeof(R), 1, STAGE_M);
+                if (threadIdx.x == 0) L = StagedLayout::make(sd.P.S, sizeof(R), STAGE_M);
                 __syncthreads();
             }
             if (!snap.go) continue;
