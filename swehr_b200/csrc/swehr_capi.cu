@@ -97,10 +97,10 @@ void swehr_set_last_error(const char *msg) { g_last_error = msg ? msg : ""; }
 
 static int64_t round_up(int64_t x, int64_t m) { return (x + m - 1) / m * m; }
 
-/* Device layout of one simulation.  A state set is, in the plain form, 9 + 2S
- * double planes in the order h hu hv vinf maxvel maxdep totm dep totsed
- * U_1..U_S M_1..M_S; in the mixed form 8 + S float planes (h hu hv maxvel
- * maxdep totm dep totsed U_1..U_S) followed by 1 + S double planes (vinf
+/* Device layout of one simulation.  A state set is, in the plain form, 10 + 2S
+ * double planes in the order h hu hv vinf maxvel maxdep totm dep totsed gz
+ * U_1..U_S M_1..M_S; in the mixed form 9 + S float planes (h hu hv maxvel
+ * maxdep totm dep totsed gz U_1..U_S) followed by 1 + S double planes (vinf
  * M_1..M_S).  Then three double z planes, the Ks plane (bulk type), rain,
  * control block, reduction partials and stage rows. */
 struct Layout {
@@ -115,7 +115,7 @@ static Layout layout_for(int nx, int ny, int S, int rnum, int has_ks, int64_t st
     L.plane = round_up((int64_t)nx * L.pitch, 32);
     L.rsize = precision == SWEHR_MIXED ? sizeof(float) : sizeof(double);
     const size_t pb = (size_t)L.plane * sizeof(double), pr = (size_t)L.plane * L.rsize;
-    L.set_bytes = precision == SWEHR_MIXED ? (size_t)(8 + S) * pr + (size_t)(1 + S) * pb : (size_t)(P_FIXED + 2 * S) * pb;
+    L.set_bytes = precision == SWEHR_MIXED ? (size_t)(9 + S) * pr + (size_t)(1 + S) * pb : (size_t)(P_FIXED + 2 * S) * pb;
     L.off_z = 2 * L.set_bytes;
     L.off_ks = L.off_z + 3 * pb;
     L.off_rain = L.off_ks + (has_ks ? pr : 0);
@@ -307,6 +307,15 @@ static int d2h_staged(swehr_ctx *c, double *host, const void *dev, size_t spitch
     return SWEHR_OK;
 }
 
+/* the lagged GZ the wave pass of step n reads, from z of step n-1 */
+static int init_gz(swehr_ctx *c, int64_t n)
+{
+    const int e = c->precision == SWEHR_MIXED ? init_gz_f32(c->P, c->B32, n, c->stream)
+                                              : init_gz_f64(c->P, c->B64, n, c->stream);
+    if (e) return set_err(SWEHR_CUDA_ERROR, std::string("init_gz: ") + cudaGetErrorString((cudaError_t)e));
+    return SWEHR_OK;
+}
+
 static int download_plane(swehr_ctx *c, double *host, PlaneRef d, cudaStream_t s)
 {
     const size_t N = (size_t)c->P.nx * c->P.ny;
@@ -339,13 +348,14 @@ static void set_views(BufsT<RS> &B, char *pool, const Layout &L, int S, int has_
             v.vinf = d + P_VINF * pl;
             v.maxvel = (RS *)(d + P_MAXVEL * pl); v.maxdep = (RS *)(d + P_MAXDEP * pl);
             v.totm = (RS *)(d + P_TOTM * pl); v.dep = (RS *)(d + P_DEP * pl); v.totsed = (RS *)(d + P_TOTSED * pl);
+            v.gz = (RS *)(d + P_GZ * pl);
             v.U = (RS *)(d + P_FIXED * pl);
             v.M = d + (P_FIXED + S) * pl;
         } else {
             RS *f = (RS *)base;
             v.h = f; v.hu = f + pl; v.hv = f + 2 * pl; v.maxvel = f + 3 * pl; v.maxdep = f + 4 * pl;
-            v.totm = f + 5 * pl; v.dep = f + 6 * pl; v.totsed = f + 7 * pl; v.U = f + 8 * pl;
-            double *d = (double *)(base + (size_t)(8 + S) * pl * sizeof(RS));
+            v.totm = f + 5 * pl; v.dep = f + 6 * pl; v.totsed = f + 7 * pl; v.gz = f + 8 * pl; v.U = f + 9 * pl;
+            double *d = (double *)(base + (size_t)(9 + S) * pl * sizeof(RS));
             v.vinf = d;
             v.M = d + pl;
         }
@@ -487,6 +497,8 @@ int swehr_ctx_create(const swehr_params *p, const swehr_inputs *in, int precisio
     if (rc) { destroy_ctx(c); return rc; }
     for (int k = 1; k < 3; k++)     /* the other two z planes from the first, on the device */
         CKC(cudaMemcpyAsync(zpl[k], zpl[0], (size_t)c->P.plane * sizeof(double), cudaMemcpyDeviceToDevice, c->stream));
+    rc = init_gz(c, 0);
+    if (rc) { destroy_ctx(c); return rc; }
     if (in->ks) {
         void *kp = precision == SWEHR_MIXED ? (void *)c->B32.ks : (void *)c->B64.ks;
         rc = upload_plane(c, PlaneRef{kp, L.rsize}, in->ks, c->stream);
@@ -783,6 +795,7 @@ extern "C" int swehr_write_field(swehr_ctx *c, int field, int k, const double *s
     if (field == SWEHR_FIELD_Z) {
         rc = upload_plane(c, z_plane(c, step), src, c->stream);
         if (!rc) rc = upload_plane(c, z_plane(c, step + 2), src, c->stream);
+        if (!rc) rc = init_gz(c, step);
     } else {
         if ((field == SWEHR_FIELD_U || field == SWEHR_FIELD_M) && (k < 1 || k > c->P.S))
             return set_err(SWEHR_INVALID, "class index out of range");

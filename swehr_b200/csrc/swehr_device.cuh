@@ -9,12 +9,14 @@
  *
  * Device layout: every field is a plane of nx rows (index i) by `pitch`
  * doubles (index j, contiguous, pitch a multiple of 32), cell (i,j) (1-based)
- * at [(i-1)*pitch + (j-1)].  A state set holds NP = 9 + 2S planes:
- *   h hu hv vinf maxvel maxdepth totm dep totsed | U_1..U_S | M_1..M_S
+ * at [(i-1)*pitch + (j-1)].  A state set holds NP = 10 + 2S planes:
+ *   h hu hv vinf maxvel maxdepth totm dep totsed gz | U_1..U_S | M_1..M_S
  * Two sets alternate between steps; the topography has three planes
  * (z of the previous, current and next step) so the lagged slopes the
  * reference's serial sweep reads (SWEHR.c:1135,1203,1243,1293,1304) can be
- * recomputed from the previous step's z.
+ * recomputed from the previous step's z.  gz of a set is the GZ the wave
+ * pass of the step reading that set uses (SWEHR.c:1279 one step late): the
+ * update writes it with the rest of the new state.
  */
 #pragma once
 #include <stdint.h>
@@ -23,7 +25,7 @@
 
 namespace swehr {
 
-enum { P_H = 0, P_HU, P_HV, P_VINF, P_MAXVEL, P_MAXDEP, P_TOTM, P_DEP, P_TOTSED, P_FIXED };
+enum { P_H = 0, P_HU, P_HV, P_VINF, P_MAXVEL, P_MAXDEP, P_TOTM, P_DEP, P_TOTSED, P_GZ, P_FIXED };
 
 /* Real-valued constants of the step in the arithmetic type R of a form
  * (double for the plain form, float for the mixed form's bulk). */

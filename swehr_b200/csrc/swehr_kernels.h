@@ -11,6 +11,7 @@ namespace swehr {
 template <class RS>
 struct SetV {
     RS *h, *hu, *hv, *maxvel, *maxdep, *totm, *dep, *totsed, *U;   /* U: S planes */
+    RS *gz;            /* GZ from this step's previous-step topography, for the wave pass */
     double *vinf, *M;                                                /* M: S planes */
 };
 
@@ -85,6 +86,10 @@ int configure_step_f32(const DevParams &P, int num_sms, StepConfig &cfg);
 int launch_step_f64(const DevParams &P, const BufsT<double> &B, Ctl *ctl, const double *rain, double *partials,
                     double *stage, double *saveflow, const StepConfig &cfg, cudaStream_t s, cudaEvent_t ev0,
                     cudaEvent_t ev1);
+/* the gz plane of the set step n reads, from its previous-step topography
+ * (at creation and after the topography is written) */
+int init_gz_f64(const DevParams &P, const BufsT<double> &B, int64_t n, cudaStream_t s);
+int init_gz_f32(const DevParams &P, const BufsT<float> &B, int64_t n, cudaStream_t s);
 int launch_step_f32(const DevParams &P, const BufsT<float> &B, Ctl *ctl, const double *rain, double *partials,
                     double *stage, double *saveflow, const StepConfig &cfg, cudaStream_t s, cudaEvent_t ev0,
                     cudaEvent_t ev1);

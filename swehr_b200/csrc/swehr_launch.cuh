@@ -44,6 +44,12 @@ struct FormLauncher {
     }
     static size_t wave_smem() { return 0; }   /* the wave pass stages nothing */
 
+    static int init_gz(const DevParams &P, const BufsT<RS> &B, int64_t n, cudaStream_t s)
+    {
+        k_init_gz<PP, RS><<<4 * 148, TILE_THREADS, 0, s>>>(P, B, n);
+        return (int)cudaGetLastError();
+    }
+
     template <int MAXS, bool BUDGET, bool SM>
     static void *update_fn() { return (void *)k_update_tile<PP, RS, MAXS, BUDGET, SM>; }
 

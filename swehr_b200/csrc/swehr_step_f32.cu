@@ -14,6 +14,11 @@ int configure_step_f32(const DevParams &P, int num_sms, StepConfig &cfg)
     return FormLauncher<PolicyF32, float>::configure(P, num_sms, cfg);
 }
 
+int init_gz_f32(const DevParams &P, const BufsT<float> &B, int64_t n, cudaStream_t s)
+{
+    return FormLauncher<PolicyF32, float>::init_gz(P, B, n, s);
+}
+
 int launch_step_f32(const DevParams &P, const BufsT<float> &B, Ctl *ctl, const double *rain, double *partials,
                     double *stage, double *saveflow, const StepConfig &cfg, cudaStream_t s, cudaEvent_t ev0,
                     cudaEvent_t ev1)

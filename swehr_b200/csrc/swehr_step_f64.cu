@@ -27,6 +27,11 @@ int configure_step_f64(const DevParams &P, int num_sms, StepConfig &cfg)
     return FormLauncher<PolicyF64, double>::configure(P, num_sms, cfg);
 }
 
+int init_gz_f64(const DevParams &P, const BufsT<double> &B, int64_t n, cudaStream_t s)
+{
+    return FormLauncher<PolicyF64, double>::init_gz(P, B, n, s);
+}
+
 int launch_step_f64(const DevParams &P, const BufsT<double> &B, Ctl *ctl, const double *rain, double *partials,
                     double *stage, double *saveflow, const StepConfig &cfg, cudaStream_t s, cudaEvent_t ev0,
                     cudaEvent_t ev1)

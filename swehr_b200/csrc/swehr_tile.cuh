@@ -457,9 +457,19 @@ __device__ __forceinline__ const RS *staged_h(const unsigned char *smb, const St
  * negated at a wall, the hard-wired inflow at j = ny+1.  Reads global memory
  * directly (no staging, no barrier): the pass is light, and a max does not
  * depend on the order the faces are visited in. */
+/* GZ of cell (i, j) from a topography plane, SWEHR.c:1279 (the wave pass's
+ * lagged GZ, computed one step ahead by the update and at initialisation) */
+template <class PP>
+__device__ __forceinline__ typename PP::R lagged_gz(const DevParams &P, const double *__restrict__ z, int i, int j)
+{
+    typedef typename PP::R R;
+    const RealC<R> &K = kc<R>(P);
+    const R sx = (R)slope_x(P, z, i, j), sy = (R)slope_y(P, z, i, j);
+    return PP::div(K.g, PP::sqrtp(sx * sx + sy * sy + 1));
+}
+
 template <class PP, class RS>
-__device__ __forceinline__ typename PP::R wave_cell(const DevParams &P, const SetV<RS> &src,
-                                                    const double *__restrict__ zp, int i, int j,
+__device__ __forceinline__ typename PP::R wave_cell(const DevParams &P, const SetV<RS> &src, int i, int j,
                                                     typename PP::R inh, typename PP::R inhv)
 {
     typedef typename PP::R R;
@@ -471,8 +481,7 @@ __device__ __forceinline__ typename PP::R wave_cell(const DevParams &P, const Se
         u = PP::div(hu, h);
         v = PP::div(hv, h);
     }
-    const R sx = (R)slope_x(P, zp, i, j), sy = (R)slope_y(P, zp, i, j);
-    const R g = PP::div(K.g, PP::sqrtp(sx * sx + sy * sy + 1));
+    const R g = (R)src.gz[q];              /* GZ of the previous step, written by its update */
     const R c = PP::sqrtp(g * h);
     R smax = 0, s;
     /* x face i+1/2 */
@@ -552,7 +561,6 @@ __global__ void __launch_bounds__(TILE_THREADS, PP::kWaveMinBlocks) k_wave_cells
     const int64_t n = ctl->step;
     const double t = ctl->t;
     const SetV<RS> src = B.set[n & 1];
-    const double *zp = B.z[(n + 2) % 3];
     double inh = 0, inhv = 0, insed = 0;
     if (P.inflow) inflow_ghost(t, inh, inhv, insed);
     /* cells in i-major order, j contiguous; (i, j) advanced by the stride */
@@ -563,7 +571,7 @@ __global__ void __launch_bounds__(TILE_THREADS, PP::kWaveMinBlocks) k_wave_cells
     int i = (int)(c0 / P.ny) + 1, j = (int)(c0 - (int64_t)(i - 1) * P.ny) + 1;
     R smax = 0;
     for (int64_t c = c0; c < total; c += stride) {
-        const R s = wave_cell<PP, RS>(P, src, zp, i, j, (R)inh, (R)inhv);
+        const R s = wave_cell<PP, RS>(P, src, i, j, (R)inh, (R)inhv);
         smax = (s > smax) ? s : smax;
         i += si;
         j += sj;
@@ -577,6 +585,20 @@ __global__ void __launch_bounds__(TILE_THREADS, PP::kWaveMinBlocks) k_wave_cells
     }
     __syncthreads();
     if (last && threadIdx.x == 0) wave_finalize(P, ctl);
+}
+
+/* the gz plane of the set step n reads, from its previous-step topography
+ * (at creation, and after the topography is written) */
+template <class PP, class RS>
+__global__ void k_init_gz(const DevParams P, const BufsT<RS> B, int64_t n)
+{
+    const SetV<RS> st = B.set[n & 1];
+    const double *zp = B.z[(n + 2) % 3];
+    const int64_t total = (int64_t)P.nx * P.ny;
+    for (int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; c < total; c += (int64_t)gridDim.x * blockDim.x) {
+        const int i = (int)(c / P.ny) + 1, j = (int)(c - (int64_t)(i - 1) * P.ny) + 1;
+        st.gz[cidx(P, i, j)] = (RS)lagged_gz<PP>(P, zp, i, j);
+    }
 }
 
 /* ---------------------------------------------------------------- update */
@@ -934,6 +956,7 @@ __device__ __forceinline__ void tile_cell(const DevParams &P, const SetV<RS> &sr
     dst.totm[q] = (RS)totm;
     dst.dep[q] = (RS)dep;
     dst.totsed[q] = (RS)totsed;
+    dst.gz[q] = (RS)gz;                /* the next step's lagged GZ: this step's topography */
     zn[q] = z;
 
     if (BUDGET) {
@@ -1318,8 +1341,7 @@ __global__ void __launch_bounds__(TILE_THREADS) k_wave_batch(const BatchHdr<RS> 
             const TileCoord tc = tile_coord(sd.P, g - sd.tile0);
             const int i = tc.i0 + (int)threadIdx.x / T_J, j = tc.j0 + (int)threadIdx.x % T_J;
             if (i <= sd.P.nx && j <= sd.P.ny) {
-                const R s = wave_cell<PP, RS>(sd.P, sd.B.set[n & 1], sd.B.z[(n + 2) % 3], i, j, (R)snap_inh,
-                                              (R)snap_inhv);
+                const R s = wave_cell<PP, RS>(sd.P, sd.B.set[n & 1], i, j, (R)snap_inh, (R)snap_inhv);
                 smax = (s > smax) ? s : smax;
             }
             run++;
