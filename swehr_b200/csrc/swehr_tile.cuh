@@ -1234,12 +1234,13 @@ __global__ void __launch_bounds__(TILE_THREADS, PP::kMinBlocks) k_update_tile(co
  * consecutive tiles of the list at a time from a global counter, so blocks
  * that start late or draw slow tiles take fewer (a fixed stride leaves the
  * whole launch waiting on the slowest block), and consecutive tiles mostly
- * share one scenario's descriptor.  Chunks are TILE_CHUNK tiles when every
- * block gets at least eight of them, else single tiles, so a small pool
- * (a serving mix of a few requests) still spreads over all blocks.  The
- * whole block calls grab_chunk; it returns false once the list is
- * exhausted. */
-#define TILE_CHUNK 4
+ * share one scenario's descriptor.  Chunks are the largest power of two up
+ * to TILE_CHUNK tiles that still gives every block at least eight of them
+ * (on 256 scenarios each doubling from 1 to 8 tiles measured faster), down
+ * to single tiles, so a small pool (a serving mix of a few
+ * requests) still spreads over all blocks.  The whole block calls
+ * grab_chunk; it returns false once the list is exhausted. */
+#define TILE_CHUNK 8
 struct TileChunk {
     int64_t g0;
     int n;
@@ -1251,7 +1252,8 @@ __device__ __forceinline__ bool grab_chunk(unsigned long long *counter, const in
 {
     __syncthreads();                                             /* the previous chunk is done with */
     if (threadIdx.x == 0) {
-        const int size = total >= (int64_t)8 * TILE_CHUNK * gridDim.x ? TILE_CHUNK : 1;
+        int size = TILE_CHUNK;
+        while (size > 1 && total < (int64_t)8 * size * gridDim.x) size >>= 1;
         const int64_t g0 = (int64_t)atomicAdd(counter, (unsigned long long)size);
         const int64_t rest = total - g0;
         ch.g0 = g0;
