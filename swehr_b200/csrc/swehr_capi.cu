@@ -769,8 +769,6 @@ extern "C" int swehr_read_field(swehr_ctx *c, int field, int k, double *dst)
     int rc = current_step(c, &step);
     if (rc) return rc;
     const int cur = (int)(step & 1);
-    const size_t N = (size_t)c->P.nx * c->P.ny;
-    const double hfilm = c->P.hfilm;
     if (field == SWEHR_FIELD_Z) {
         rc = download_plane(c, dst, z_plane(c, step), c->stream);
     } else if (field == SWEHR_FIELD_VEL || field == SWEHR_FIELD_SED) {
