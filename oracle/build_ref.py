@@ -1,7 +1,8 @@
 """Build the reference SWEHR program into oracle/_ref/ (TEST INFRASTRUCTURE).
 
-Reads SWEHR.c from the reference checkout (default /root/reference, or
-$SWEHR_REFERENCE), applies the small set of patches below, writes the patched
+Reads SWEHR.c from the reference checkout named by --reference or by the
+environment variable SWEHR_REFERENCE (no default: a missing checkout is an
+error), applies the small set of patches below, writes the patched
 copy to oracle/_ref/swehr_ref.c and compiles two binaries:
 
   oracle/_ref/swehr_ref      serial, exactly the reference's arithmetic
@@ -25,7 +26,7 @@ program anyway):
   4. After the loop: elapsed time via omp_get_wtime, step count, and a
      %.17g dump of every state field to swehr_dump.txt.
 
-Run:  python oracle/build_ref.py [--reference DIR]
+Run:  SWEHR_REFERENCE=<checkout> python oracle/build_ref.py   (or --reference DIR)
 """
 import argparse
 import os
@@ -188,11 +189,25 @@ def build(reference: str, quiet: bool = False) -> bool:
     return True
 
 
+REFERENCE_ENV = "SWEHR_REFERENCE"
+
+
+def reference_dir(explicit: str = None) -> str:
+    """The reference checkout: `explicit`, else $SWEHR_REFERENCE; raises
+    with a clear message when neither names a directory holding SWEHR.c."""
+    d = explicit or os.environ.get(REFERENCE_ENV)
+    if not d:
+        raise SystemExit(f"build_ref: no reference checkout given: pass --reference DIR or set {REFERENCE_ENV}")
+    if not os.path.exists(os.path.join(d, "SWEHR.c")):
+        raise SystemExit(f"build_ref: {d} holds no SWEHR.c")
+    return d
+
+
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--reference", default=os.environ.get("SWEHR_REFERENCE", "/root/reference"))
+    ap.add_argument("--reference", default=None, help=f"reference checkout (default: ${REFERENCE_ENV})")
     a = ap.parse_args()
-    ok = build(a.reference)
+    ok = build(reference_dir(a.reference))
     sys.exit(0 if ok else 1)
 
 

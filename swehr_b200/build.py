@@ -39,7 +39,7 @@ def nvcc() -> str:
 
 def build(verbose: bool = False, ptxas_v: bool = False) -> str:
     os.makedirs(BUILD, exist_ok=True)
-    objs = []
+    objs, jobs = [], []
     for src, extra in SOURCES:
         obj = os.path.join(BUILD, os.path.splitext(src)[0] + ".o")
         srcp = os.path.join(CSRC, src)
@@ -51,13 +51,18 @@ def build(verbose: bool = False, ptxas_v: bool = False) -> str:
                 cmd += ["-Xptxas", "-v"]
             if verbose:
                 print(" ".join(cmd))
-            r = subprocess.run(cmd, capture_output=True, text=True)
-            if r.returncode != 0:
-                sys.stderr.write(r.stdout + r.stderr)
-                raise RuntimeError(f"nvcc failed on {src}")
-            if ptxas_v:
-                sys.stdout.write(r.stderr)
+            jobs.append((src, cmd))
         objs.append(obj)
+    # the translation units are independent: compile them side by side
+    from concurrent.futures import ThreadPoolExecutor
+    with ThreadPoolExecutor(max_workers=max(1, min(len(jobs), os.cpu_count() or 1))) as ex:
+        results = list(ex.map(lambda j: (j[0], subprocess.run(j[1], capture_output=True, text=True)), jobs))
+    for src, r in results:
+        if r.returncode != 0:
+            sys.stderr.write(r.stdout + r.stderr)
+            raise RuntimeError(f"nvcc failed on {src}")
+        if ptxas_v:
+            sys.stdout.write(r.stderr)
     cmd = [nvcc()] + ARCH + ["-shared", "-o", OUT] + objs + ["-lcudart"]
     if verbose:
         print(" ".join(cmd))

@@ -264,6 +264,9 @@ static void stage_out(double *dst, const void *src, size_t n, size_t esize)
     for (int t = 0; t < T - 1; t++) th[t].join();
 }
 
+static int d2h_staged_copy(swehr_ctx *c, double *host, const void *dev, size_t spitch, size_t esize,
+                           int64_t nrows, int64_t ncols);
+
 static int d2h_staged(swehr_ctx *c, double *host, const void *dev, size_t spitch, size_t esize, int64_t nrows,
                       int64_t ncols, int *done)
 {
@@ -278,6 +281,22 @@ static int d2h_staged(swehr_ctx *c, double *host, const void *dev, size_t spitch
     if (!c->ev_stage[0])
         for (int e = 0; e < 2; e++) CK(cudaEventCreateWithFlags(&c->ev_stage[e], cudaEventDisableTiming));
     c->h_stage = stage;
+    const int rc = d2h_staged_copy(c, host, dev, spitch, esize, nrows, ncols);
+    if (rc != SWEHR_OK) {
+        /* a copy into the shared pinned pair may still be in flight: let it
+         * land before the lock is released and the next reader reuses the pair */
+        cudaStreamSynchronize(c->stream);
+        return rc;
+    }
+    *done = 1;
+    return SWEHR_OK;
+}
+
+/* the chunked copy of d2h_staged (its lock held, the pinned pair set up) */
+static int d2h_staged_copy(swehr_ctx *c, double *host, const void *dev, size_t spitch, size_t esize,
+                           int64_t nrows, int64_t ncols)
+{
+    const size_t row_in = (size_t)ncols * esize;
     const int64_t per = (int64_t)(kStageBytes / row_in);
     int64_t prev_r0 = -1, prev_n = 0;
     int prev_b = 0;
@@ -303,7 +322,6 @@ static int d2h_staged(swehr_ctx *c, double *host, const void *dev, size_t spitch
         stage_out(host + (size_t)prev_r0 * ncols, (char *)c->h_stage + (size_t)prev_b * kStageBytes,
                   (size_t)prev_n * ncols, esize);
     }
-    *done = 1;
     return SWEHR_OK;
 }
 

@@ -34,7 +34,7 @@
 #include <string>
 
 #include "../../include/swehr.h"
-#include "swehr_faces.cuh"
+#include "swehr_tile.cuh"
 
 namespace swehr {
 
@@ -49,56 +49,23 @@ __global__ void __launch_bounds__(NB_THREADS) k_cfl_noalloc(const DevParams P, c
                                                              const double *__restrict__ zp, double t,
                                                              double *scratch, double *result)
 {
-    /* The wave pass reads a state set (planes h, hu, hv) and the previous
-     * step's z; here the caller's planes are addressed through a Bufs-like
-     * view with plane stride 0 and separate bases. */
+    /* The faces each cell owns and their wave speeds are those of the
+     * stepping path's wave pass (wave_cell_g, one definition); only the
+     * cell's lagged GZ comes from the caller's previous-step topography
+     * instead of the state's GZ plane. */
     double inh = 0, inhv = 0, insed = 0;
     if (P.inflow) inflow_ghost(t, inh, inhv, insed);
+    SetV<double> src{};
+    src.h = const_cast<double *>(h);
+    src.hu = const_cast<double *>(hu);
+    src.hv = const_cast<double *>(hv);
     const int64_t total = (int64_t)P.nx * P.ny;
     const int64_t first = (int64_t)blockIdx.x * NOALLOC_CELLS_PER_BLOCK;
     double smax = 0;
     for (int64_t c = first + threadIdx.x; c < first + NOALLOC_CELLS_PER_BLOCK && c < total; c += blockDim.x) {
         const int i = (int)(c / P.ny) + 1, j = (int)(c % P.ny) + 1;
-        /* faces owned by this cell: i+1/2, j+1/2, and the boundary faces 1/2 */
-        for (int f = 0; f < 4; f++) {
-            if (f == 2 && i != 1) continue;
-            if (f == 3 && j != 1) continue;
-            const bool xface = (f == 0 || f == 2);
-            const int iL = (f == 2) ? 0 : i, jL = (f == 3) ? 0 : j;
-            double hl, hr, ul, ur, vl, vr, g;
-            if (xface) {
-                const int li = iL == 0 ? 1 : iL, ri = iL + 1 > P.nx ? P.nx : iL + 1;
-                const int64_t ql = cidx(P, li, j), qr = cidx(P, ri, j);
-                hl = h[ql]; ul = hu[ql]; vl = hv[ql];
-                hr = h[qr]; ur = hu[qr]; vr = hv[qr];
-                if (iL == 0 && P.bndry[0] == 1) ul = -ul;
-                if (iL + 1 > P.nx && P.bndry[2] == 1) ur = -ur;
-                g = gz_of(P, zp, li, j);
-                double T0, T1, T2;
-                double s = hllc(hl, hr, ul, ur, vl, vr, g, P.hfilm, T0, T1, T2);
-                if (s > smax) smax = s;
-            } else {
-                const int lj = jL == 0 ? 1 : jL;
-                const int64_t ql = cidx(P, i, lj);
-                hl = h[ql]; ul = hv[ql]; vl = hu[ql];
-                if (jL == 0 && P.bndry[1] == 1) ul = -ul;
-                if (jL + 1 > P.ny) {
-                    if (P.inflow) { hr = inh; ur = inhv; vr = 0; }
-                    else {
-                        const int64_t qr = cidx(P, i, P.ny);
-                        hr = h[qr]; ur = hv[qr]; vr = hu[qr];
-                        if (P.bndry[3] == 1) ur = -ur;
-                    }
-                } else {
-                    const int64_t qr = cidx(P, i, jL + 1);
-                    hr = h[qr]; ur = hv[qr]; vr = hu[qr];
-                }
-                g = gz_of(P, zp, i, lj);
-                double T0, T1, T2;
-                double s = hllc(hl, hr, ul, ur, vl, vr, g, P.hfilm, T0, T1, T2);
-                if (s > smax) smax = s;
-            }
-        }
+        const double s = wave_cell_g<PolicyF64, double>(P, src, i, j, inh, inhv, lagged_gz<PolicyF64>(P, zp, i, j));
+        smax = (s > smax) ? s : smax;
     }
     __shared__ double red[NB_THREADS / 32];
     __shared__ bool last;
@@ -152,6 +119,9 @@ extern "C" int swehr_cfl_noalloc(const swehr_params *p, const double *d_h, const
         return noalloc_err(SWEHR_INVALID, "swehr_cfl_noalloc: NULL argument");
     if (p->nx < 2 || p->ny < 2 || pitch < p->ny)
         return noalloc_err(SWEHR_INVALID, "swehr_cfl_noalloc: need nx, ny >= 2 and pitch >= ny");
+    /* the kernel indexes rows with a 32-bit pitch: nx rows of it must stay addressable */
+    if (pitch > INT32_MAX || (int64_t)p->nx > INT64_MAX / pitch)
+        return noalloc_err(SWEHR_INVALID, "swehr_cfl_noalloc: pitch exceeds INT32_MAX (or nx*pitch overflows)");
     if ((int64_t)p->nx * p->ny > SWEHR_NOALLOC_MAX_CELLS)
         return noalloc_err(SWEHR_INVALID, "swehr_cfl_noalloc: nx*ny exceeds SWEHR_NOALLOC_MAX_CELLS (16777216), "
                                           "the size its fixed scratch array can reduce");
@@ -178,6 +148,7 @@ extern "C" int swehr_cfl_noalloc(const swehr_params *p, const double *d_h, const
     for (int k = 0; k < 4; k++) P.bndry[k] = p->bndry[k];
     P.dx = p->dx; P.oneoverdx = 1 / p->dx; P.half_odx = 0.5 * P.oneoverdx; P.tend = p->tend;
     P.g = p->g; P.hfilm = p->hfilm; P.cstable = p->cstable; P.maxstep = p->maxstep;
+    P.kd.g = p->g; P.kd.hfilm = p->hfilm;   /* the constants the per-cell wave routine reads */
     cudaStream_t s = (cudaStream_t)stream;
     const int64_t total = (int64_t)p->nx * p->ny;
     const int grid = (int)((total + NOALLOC_CELLS_PER_BLOCK - 1) / NOALLOC_CELLS_PER_BLOCK);

@@ -468,9 +468,10 @@ __device__ __forceinline__ typename PP::R lagged_gz(const DevParams &P, const do
     return PP::div(K.g, PP::sqrtp(sx * sx + sy * sy + 1));
 }
 
+/* wave_cell with the cell's lagged GZ given (g) */
 template <class PP, class RS>
-__device__ __forceinline__ typename PP::R wave_cell(const DevParams &P, const SetV<RS> &src, int i, int j,
-                                                    typename PP::R inh, typename PP::R inhv)
+__device__ __forceinline__ typename PP::R wave_cell_g(const DevParams &P, const SetV<RS> &src, int i, int j,
+                                                      typename PP::R inh, typename PP::R inhv, typename PP::R g)
 {
     typedef typename PP::R R;
     const RealC<R> &K = kc<R>(P);
@@ -481,7 +482,6 @@ __device__ __forceinline__ typename PP::R wave_cell(const DevParams &P, const Se
         u = PP::div(hu, h);
         v = PP::div(hv, h);
     }
-    const R g = (R)src.gz[q];              /* GZ of the previous step, written by its update */
     const R c = PP::sqrtp(g * h);
     R smax = 0, s;
     /* x face i+1/2 */
@@ -518,6 +518,14 @@ __device__ __forceinline__ typename PP::R wave_cell(const DevParams &P, const Se
         smax = (s > smax) ? s : smax;
     }
     return smax;
+}
+
+template <class PP, class RS>
+__device__ __forceinline__ typename PP::R wave_cell(const DevParams &P, const SetV<RS> &src, int i, int j,
+                                                    typename PP::R inh, typename PP::R inhv)
+{
+    /* GZ of the previous step, written by its update */
+    return wave_cell_g<PP, RS>(P, src, i, j, inh, inhv, (typename PP::R)src.gz[cidx(P, i, j)]);
 }
 
 /* block maximum of the threads' partial maxima (result valid in thread 0) */

@@ -22,7 +22,7 @@ Each file holds the Case (params as JSON, topo, rain, ds, pfrac, ks) and the
 reference's %.17g dump of every state field.
 
 Run (needs the reference checkout; it is not read anywhere else):
-    python tests/golden/make_golden.py [--reference /root/reference]
+    SWEHR_REFERENCE=<checkout> python tests/golden/make_golden.py   (or --reference DIR)
 """
 import argparse
 import json
@@ -124,11 +124,12 @@ def shipped_files(reference):
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--reference", default="/root/reference")
+    ap.add_argument("--reference", default=None, help="reference checkout (default: $SWEHR_REFERENCE)")
     ap.add_argument("--only", default=None, help="shipped_files: only regenerate that fixture")
     a = ap.parse_args()
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import build_ref
+    a.reference = build_ref.reference_dir(a.reference)
     if not build_ref.build(a.reference):
         raise SystemExit("reference not available")
     if a.only == "shipped_files":

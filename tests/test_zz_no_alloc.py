@@ -67,7 +67,7 @@ def _noalloc_dt(L, rt, sim, zprev, t):
             b.free()
 
 
-@pytest.mark.parametrize("which", ["fractal", "shipped_inflow"])
+@pytest.mark.parametrize("which", ["fractal", "shipped_inflow", "walls_odd"])
 def test_noalloc_cfl_matches_stepping_path_two_calls(which):
     from swehr_b200.lib import Simulation, load
     from harness import load_golden
@@ -76,6 +76,11 @@ def test_noalloc_cfl_matches_stepping_path_two_calls(which):
     if which == "fractal":
         case = W.fractal_domain(nx=300, ny=170, dx=2.0, steps=100)
         warm = 40
+    elif which == "walls_odd":
+        # every side a wall, sizes that fill no block or tile evenly
+        case = W.fractal_domain(nx=131, ny=77, dx=2.0, steps=100)
+        case.params["bndry"] = (1, 1, 1, 1)
+        warm = 60
     else:
         case, _ = load_golden("shipped")
         warm = 500
@@ -103,3 +108,6 @@ def test_noalloc_rejects_oversize_and_bad_arguments():
     p = make_params(nx=8, ny=8, dx=1.0, tend=10.0, rnum=1, rint=1.0, sclass=1)
     assert L.swehr_cfl_noalloc(C.byref(p), fake, fake, fake, fake, 4, 0.0, fake, None) == 5   # pitch < ny
     assert L.swehr_cfl_noalloc(C.byref(p), None, fake, fake, fake, 8, 0.0, fake, None) == 5
+    # a pitch the kernel's 32-bit row stride cannot hold
+    assert L.swehr_cfl_noalloc(C.byref(p), fake, fake, fake, fake, 2 ** 31, 0.0, fake, None) == 5
+    assert b"INT32_MAX" in L.swehr_last_error()
