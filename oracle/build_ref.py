@@ -25,6 +25,12 @@ program anyway):
      (SWEHR.c:699, 710-715 read out of bounds when ny < 50).
   4. After the loop: elapsed time via omp_get_wtime, step count, and a
      %.17g dump of every state field to swehr_dump.txt.
+  5. The deposit cohesion (SWEHR.c:647) and an interior SOLID mask
+     (solid.txt, nx*ny integers i-major; the stock program leaves SOLID all
+     zero, SWEHR.c:597) come from swehr_ref.cfg as well, so slope failure
+     and interior walls can be exercised.  Every int matrix gets one spare
+     zero row: the y-face solid test reads SOLID[nx][ny+1], one element past
+     the stock allocation (SWEHR.c:1206,1211).
 
 Run:  SWEHR_REFERENCE=<checkout> python oracle/build_ref.py   (or --reference DIR)
 """
@@ -49,6 +55,10 @@ static double swehr_cfg_thetas = 0.4, swehr_cfg_hf = 0.001, swehr_cfg_vinf0 = 1e
 static double swehr_cfg_uc = 0, swehr_cfg_uc2 = 0;
 static int swehr_cfg_ksfile = 0;
 static double *swehr_cfg_ksvals = 0;
+static int swehr_cfg_set_cohesion = 0;
+static double swehr_cfg_cohesion = 400;
+static int swehr_cfg_solidfile = 0;
+static int *swehr_cfg_solidvals = 0;
 static long swehr_steps = 0;
 static void swehr_cfg_load(void)
 {
@@ -77,6 +87,8 @@ static void swehr_cfg_load(void)
         else if (!strcmp(key, "vinf0")) swehr_cfg_vinf0 = v;
         else if (!strcmp(key, "uc")) swehr_cfg_uc = v;
         else if (!strcmp(key, "uc2")) swehr_cfg_uc2 = v;
+        else if (!strcmp(key, "cohesion")) { swehr_cfg_cohesion = v; swehr_cfg_set_cohesion = 1; }
+        else if (!strcmp(key, "solidfile")) swehr_cfg_solidfile = (int)v;
     }
     fclose(f);
 }
@@ -94,6 +106,21 @@ static double swehr_cfg_ks_at(int i, int j, int nx, int ny)
         fclose(f);
     }
     return swehr_cfg_ksvals[(long)(i - 1) * ny + (j - 1)];
+}
+static int swehr_cfg_solid_at(int i, int j, int nx, int ny)
+{
+    swehr_cfg_load();
+    if (!swehr_cfg_solidfile) return 0;
+    if (!swehr_cfg_solidvals) {
+        FILE *f = fopen("./solid.txt", "r");
+        long n, q;
+        n = (long)nx * ny;
+        swehr_cfg_solidvals = (int *)calloc(n, sizeof(int));
+        for (q = 0; q < n; q++)
+            if (fscanf(f, "%d", &swehr_cfg_solidvals[q]) != 1) break;
+        fclose(f);
+    }
+    return swehr_cfg_solidvals[(long)(i - 1) * ny + (j - 1)];
 }
 '''
 
@@ -123,6 +150,13 @@ DUMP = r'''
 PATCHES = [
     ("#include<stdlib.h>\n", "#include<stdlib.h>\n#include<string.h>\n", 1),
     ("malloc(", "calloc(1,", None),
+    # one spare row of zeros behind every int matrix: the y-face solid test
+    # reads SOLID[i][ny+1] (SWEHR.c:1206,1211), one int past the allocation at i = nx
+    ("(nrow*ncol+NR_END)*sizeof(int)", "(nrow*ncol+NR_END+ncol)*sizeof(int)", 1),
+    ("            fscanf(fr0,\"%lf\",&TOPO[i][j]);      // TOPOGRAPHY\n",
+     "            fscanf(fr0,\"%lf\",&TOPO[i][j]);      // TOPOGRAPHY\n"
+     "            SOLID[i][j]=swehr_cfg_solid_at(i,j,nx,ny);\n", 1),
+    ("    cohesion=400;", "    cohesion=400; swehr_cfg_load(); if (swehr_cfg_set_cohesion) cohesion=swehr_cfg_cohesion;", 1),
     ("void initialcondition(", HELPERS + "\nvoid initialcondition(", 1),
     ("            MANNING[i][j]=0.1;", "            swehr_cfg_load();\n            MANNING[i][j]=swehr_cfg_roughness;", 1),
     ("            ROUGHNESS[i][j]=0.1;", "            ROUGHNESS[i][j]=swehr_cfg_roughness;", 1),

@@ -90,6 +90,11 @@ typedef struct orc_ctx {
     /* budget */
     double b_rain, b_out, b_clamp, b_bulk, b_inf, b_water0;
     double b_det[SWEHR_MAX_CLASSES], b_sout[SWEHR_MAX_CLASSES], b_sed0[SWEHR_MAX_CLASSES];
+    /* branch counters over the run (cell-steps), read by the tests to show a
+     * case exercises them: slope failure (SWEHR.c:1295-1311), the debris-flow
+     * forcing (DFMASK > 0, SWEHR.c:1315-1316) and the debris-flow override of
+     * every source (SWEHR.c:1392-1400) */
+    int64_t n_fail, n_dfmask, n_debris;
 } orc_ctx;
 
 #define IDX(c, i, j) (((size_t)(i) - 1) * (size_t)(c)->ny + ((size_t)(j) - 1))
@@ -283,7 +288,8 @@ static int orc_step(orc_ctx *c)
     }
 
     /* phase 3: sources from the state at the start of the step (SWEHR.c:1233-1401) */
-#pragma omp parallel for schedule(static)
+    int64_t n_fail = 0, n_dfmask = 0, n_debris = 0;
+#pragma omp parallel for schedule(static) reduction(+ : n_fail, n_dfmask, n_debris)
     for (int i = 1; i <= nx; i++)
         for (int j = 1; j <= ny; j++) {
             size_t q = IDX(c, i, j);
@@ -331,6 +337,9 @@ static int orc_step(orc_ctx *c)
             double betay = -(1 - p->lambda) * gz * h * p->frictionangle;
             if (hu < 0) betax = -1 * betax;
             if (hv < 0) betay = -1 * betay;
+            n_fail += fail == 1;
+            n_dfmask += dfmask > 0;
+            n_debris += (h > 9 * p->h0 && totsed > p->cthreshold);
             double *sf = c->srcf + q * 9;
             sf[0] = SXf; sf[1] = SYf; sf[2] = gammax; sf[3] = gammay; sf[4] = dfmask;
             sf[5] = betax; sf[6] = betay; sf[7] = fail; sf[8] = gz;
@@ -375,6 +384,10 @@ static int orc_step(orc_ctx *c)
                 c->VF[(size_t)k * N + q] = VF;
             }
         }
+
+    c->n_fail += n_fail;
+    c->n_dfmask += n_dfmask;
+    c->n_debris += n_debris;
 
     /* CFL time step (SWEHR.c:1409-1413) */
     double dt = p->cstable * p->dx / smax;
@@ -709,6 +722,13 @@ int orc_get_budget(orc_ctx *c, swehr_budget *b)
 }
 
 double orc_time(orc_ctx *c) { return c->t; }
+
+/* branch counters: 0 slope failures, 1 cells with debris forcing (DFMASK > 0),
+ * 2 cells under the debris-flow override; cell-steps since creation */
+int64_t orc_counter(orc_ctx *c, int which)
+{
+    return which == 0 ? c->n_fail : which == 1 ? c->n_dfmask : which == 2 ? c->n_debris : -1;
+}
 int64_t orc_steps(orc_ctx *c) { return c->steps; }
 
 int orc_threads(void)

@@ -48,6 +48,8 @@ def write_inputs(case, directory: str) -> None:
     np.savetxt(os.path.join(directory, "topoin.txt"), case.topo.reshape(-1), fmt="%.17g")
     if case.ks is not None:
         np.savetxt(os.path.join(directory, "ks.txt"), case.ks.reshape(-1), fmt="%.17g")
+    if getattr(case, "solid", None) is not None:
+        np.savetxt(os.path.join(directory, "solid.txt"), case.solid.reshape(-1).astype(np.int64), fmt="%d")
 
 
 def write_ref_cfg(case, directory: str, max_steps: int = -1, movies: int = 0) -> None:
@@ -62,6 +64,8 @@ def write_ref_cfg(case, directory: str, max_steps: int = -1, movies: int = 0) ->
         f"theta0 {p.get('theta0', 0.05)!r}", f"thetas {p.get('thetas', 0.4)!r}",
         f"hf {p.get('hf', 0.001)!r}", f"vinf0 {p.get('vinf0', 1e-4)!r}",
         f"uc {p.get('uc', 0.0)!r}", f"uc2 {p.get('uc2', 0.0)!r}",
+        f"cohesion {p.get('cohesion', 400.0)!r}",
+        f"solidfile {1 if getattr(case, 'solid', None) is not None else 0}",
     ]
     with open(os.path.join(directory, "swehr_ref.cfg"), "w") as f:
         f.write("\n".join(lines) + "\n")

@@ -12,6 +12,9 @@ text files written by swehr_b200.io) and the GPU read identical bits.
   ensemble()         256 square catchments of side 64-1024 (log-uniform)
   storm_domain()     8192x8192 fractal domain with a moving Gaussian storm
   tiny_case()        small random grids for parity tests
+  failure_tiny(), failure_hillslope()
+                     cross-sloped grids with the deposit cohesion lowered,
+                     so the slope-failure branch fires
 """
 from __future__ import annotations
 
@@ -191,3 +194,29 @@ def tiny_case(nx: int = 12, ny: int = 9, S: int = 3, seed: int = 5, bndry=(0, 1,
                          bndry=tuple(bndry), inflow=inflow)
     params.update(over)
     return Case(f"tiny{nx}x{ny}s{S}", params, topo, rain, ds, pf, ks=ks)
+
+
+def failure_tiny(slope_y: float = 0.5, cohesion: float = 5.0, **kw) -> Case:
+    """tiny_case tilted across the slope (z += slope_y * y) with the deposit
+    cohesion lowered from the reference's 400 Pa: the slope-failure test
+    (SWEHR.c:1292-1312) then fires in many cells and moves deposited mass
+    back into suspension (SWEHR.c:1497-1503)."""
+    c = tiny_case(**kw)
+    y = (np.arange(1, c.ny + 1) - 1) * float(c.params["dx"])
+    c.topo = c.topo + slope_y * y[None, :]
+    c.params["cohesion"] = cohesion
+    c.name = f"failure{c.nx}x{c.ny}s{c.sclass}"
+    return c
+
+
+def failure_hillslope(cross: float = 0.4, cohesion: float = 20.0, tend: float = 600.0) -> Case:
+    """The 200x50 hillslope with a cross slope (z += cross * y), cohesion
+    lowered to `cohesion` Pa, run to `tend`: slope failure in ~1.5 % of the
+    cell-steps, deposits and resuspension over the whole event."""
+    c = hillslope200x50()
+    y = (np.arange(1, c.ny + 1) - 1) * float(c.params["dx"])
+    c.topo = c.topo + cross * y[None, :]
+    c.params["cohesion"] = cohesion
+    c.params["tend"] = tend
+    c.name = "failure_hillslope200x50"
+    return c

@@ -12,6 +12,9 @@ oracle/build_ref.py, on:
                     on and off, per-cell Ks, to the end of their event
   hillslope.npz     the 200x50 hillslope, full 1200 s run, and the state at
                     600 s (mid-event, wet)
+  failure_*.npz     cross-sloped grids with the deposit cohesion lowered
+                    (two small ones and the 200x50 hillslope to 600 s):
+                    slope failure fires (SWEHR.c:1292-1312, 1497-1503)
   shipped_files.npz the reference's own output files for the shipped
                     example run as shipped (movies on): the ten result
                     grids, stage.txt, saveflow.txt, every 30th frame of the
@@ -46,6 +49,11 @@ TINY = [
     dict(nx=15, ny=11, S=4, seed=7, bndry=(0, 0, 0, 0), inflow=0, rain_mmh=300.0, tend=120.0),
     dict(nx=9, ny=14, S=2, seed=8, bndry=(1, 1, 1, 1), inflow=1, rain_mmh=200.0, tend=90.0, per_cell_ks=False),
     dict(nx=20, ny=6, S=7, seed=9, bndry=(0, 1, 0, 1), inflow=0, rain_mmh=500.0, tend=150.0),
+]
+
+FAILURE = [
+    dict(slope_y=0.5, cohesion=5.0, nx=20, ny=16, S=4, seed=31, bndry=(0, 1, 1, 1), rain_mmh=300.0, tend=120.0),
+    dict(slope_y=0.7, cohesion=50.0, nx=17, ny=13, S=7, seed=32, bndry=(1, 1, 0, 0), rain_mmh=200.0, tend=150.0),
 ]
 
 DUMP_KEYS = ("h", "hu", "hv", "z", "vinf", "totm", "dep", "totsed", "maxvel", "maxdepth", "U", "M", "sed",
@@ -122,10 +130,22 @@ def shipped_files(reference):
     print("wrote", path, os.path.getsize(path), "bytes")
 
 
+def failure_fixtures():
+    for n, kw in enumerate(FAILURE):
+        c = W.failure_tiny(**kw)
+        c.params["bndry"] = list(c.params["bndry"])
+        d, _ = harness.run_reference(c)
+        save(os.path.join(HERE, f"failure_{n}.npz"), c, {"end": d})
+    c = W.failure_hillslope()
+    c.params["bndry"] = list(c.params["bndry"])
+    d, _ = harness.run_reference(c)
+    save(os.path.join(HERE, "failure_hillslope.npz"), c, {"end": d})
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--reference", default=None, help="reference checkout (default: $SWEHR_REFERENCE)")
-    ap.add_argument("--only", default=None, help="shipped_files: only regenerate that fixture")
+    ap.add_argument("--only", default=None, help="shipped_files | failure: only regenerate those fixtures")
     a = ap.parse_args()
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import build_ref
@@ -135,6 +155,10 @@ def main():
     if a.only == "shipped_files":
         shipped_files(a.reference)
         return
+    if a.only in (None, "failure"):
+        failure_fixtures()
+        if a.only == "failure":
+            return
     c = shipped_case(a.reference)
     d1, _ = harness.run_reference(c, max_steps=2000)
     d2, _ = harness.run_reference(c, max_steps=20000)

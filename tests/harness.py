@@ -74,6 +74,8 @@ class OracleRun:
             L.orc_steps.restype = C.c_int64
             L.orc_steps.argtypes = [C.c_void_p]
             L.orc_threads.restype = C.c_int
+            L.orc_counter.restype = C.c_int64
+            L.orc_counter.argtypes = [C.c_void_p, C.c_int]
             for fn in ("orc_m_pow",):
                 getattr(L, fn).restype = C.c_double
                 getattr(L, fn).argtypes = [C.c_double, C.c_double]
@@ -104,6 +106,11 @@ class OracleRun:
     @property
     def steps(self):
         return self.L.orc_steps(self.ctx)
+
+    def counters(self) -> dict:
+        """Cell-steps so far that took a rare branch: slope failure, debris
+        forcing (DFMASK > 0), the debris-flow override of every source."""
+        return {n: int(self.L.orc_counter(self.ctx, k)) for k, n in enumerate(("fail", "dfmask", "debris"))}
 
     def field(self, name: str, k: int = 0) -> np.ndarray:
         out = np.empty((self.case.nx, self.case.ny))

@@ -20,6 +20,12 @@ def _bitexact(a, b, names=FIELDS):
     return {k: v for k, v in res.items() if not v[2]}
 
 
+# the inflow cases carry the hard-wired 500 kg/m^3 ghost concentration of
+# every class into the domain: TOTSED passes 0.2 (debris forcing, SWEHR.c:
+# 1315-1316) and 0.4 (the debris-flow override, SWEHR.c:1392-1400)
+DEBRIS_TINY = {1: ("dfmask", "debris"), 3: ("dfmask",)}
+
+
 @pytest.mark.parametrize("n", range(5))
 def test_glibc_oracle_matches_reference_tiny(n):
     case, dumps = load_golden(f"tiny_{n}")
@@ -28,10 +34,30 @@ def test_glibc_oracle_matches_reference_tiny(n):
     d = dumps["end"]
     assert o.steps == d["steps"] and o.t == d["t"]
     assert not _bitexact(o.fields(), d)
+    for branch in DEBRIS_TINY.get(n, ()):
+        assert o.counters()[branch] > 0, (n, branch, o.counters())
     st, sf = o.series()
     assert np.array_equal(st, d["stage"], equal_nan=True)
     # the reference clamps its sample points into the grid; compare the points that are inside
     assert st.shape[0] == d["saveflow"].shape[0]
+
+
+@pytest.mark.parametrize("name", ["failure_0", "failure_1", "failure_hillslope"])
+def test_glibc_oracle_matches_reference_slope_failure(name):
+    """Cross-sloped grids with the deposit cohesion lowered: the slope
+    failure test fires (SWEHR.c:1292-1312) and the class loop moves 99 % of
+    the deposit into suspension and zeroes TOTM and DEP (SWEHR.c:1497-1503);
+    the oracle still matches the reference bit for bit."""
+    case, dumps = load_golden(name)
+    o = OracleRun(case, "glibc")
+    o.advance()
+    d = dumps["end"]
+    assert o.steps == d["steps"] and o.t == d["t"]
+    assert not _bitexact(o.fields(), d)
+    n = o.counters()
+    assert n["fail"] > 0, n
+    st, _ = o.series()
+    assert np.array_equal(st, d["stage"], equal_nan=True)
 
 
 def test_glibc_oracle_matches_reference_shipped_example():
