@@ -24,7 +24,7 @@
 extern "C" {
 #endif
 
-#define SWEHR_ABI_VERSION 1
+#define SWEHR_ABI_VERSION 2
 #define SWEHR_MAX_CLASSES 16
 
 typedef enum swehr_status {
@@ -94,6 +94,14 @@ typedef struct swehr_inputs {
     const double *ds;       /* sclass diameters [m] (particlesizein.txt) */
     const double *pfrac;    /* sclass mass fractions of the original soil (particlepercentin.txt) */
     const double *ks;       /* optional nx*ny saturated conductivity [m/s]; NULL -> params.ks everywhere */
+    /* optional nx*ny interior solid mask, i-major (SOLID[i][j], SWEHR.c:597; the
+     * stock program leaves it all zero): a nonzero cell is outside the flow
+     * domain.  swehr_create fills its topography from its neighbours as
+     * initialcondition does (SWEHR.c:288-322), faces between a solid and a flow
+     * cell reflect the flow cell's state (SWEHR.c:1137-1146, 1205-1214), and a
+     * solid cell takes no sources and holds no water or suspended sediment
+     * (SWEHR.c:1233, 1421, 1566-1574).  NULL -> no solid cells.  (Added in ABI 2.) */
+    const int32_t *solid;
 } swehr_inputs;
 
 /* Fields readable with swehr_read_field; all are nx*ny, i-major. */

@@ -32,9 +32,18 @@
  * SOLID and TRACER before writing them (SWEHR.c:248, 1285, 1293, 1332);
  * fresh heap pages are zero there, and they are zero here.
  *
+ * Interior solid cells (an optional SOLID mask; the stock program leaves
+ * it zero): the topography fill of initialcondition (SWEHR.c:288-322), the
+ * reflecting fluxes at solid/flow faces (SWEHR.c:1137-1146, 1205-1214), no
+ * sources in solid cells (SWEHR.c:1233) -- so their slopes and GZ keep the
+ * setup values their neighbours then read -- and zero water and suspended
+ * sediment there (SWEHR.c:1566-1574).  NEARSOLIDX/Y only select the
+ * reconstruction order near solid cells, and the order is first everywhere
+ * (order=1, SWEHR.c:635), so they change nothing and are not kept.
+ *
  * Left out because nothing observable depends on them: TRACER (only feeds
  * its own flux, never an output), UOLD/VELOLD/TOPOOLD/D/FAILCNT/BEDFLUX*
- * (write-only), and interior SOLID cells (SOLID is all zero in the reference).
+ * (write-only).
  */
 #include <math.h>
 #include <stdint.h>
@@ -72,6 +81,8 @@ typedef struct orc_ctx {
     int nx, ny, S, N;
     double *h, *hu, *hv, *z, *zp, *vinf, *maxvel, *maxdep, *totm, *dep, *totsed, *rho, *ks;
     double *U, *M, *sed;          /* class-major: [k*N + c] */
+    int32_t *solid;               /* interior solid mask (SOLID, SWEHR.c:597), NULL when none */
+    double *sx0, *sy0, *gz0;      /* setup slopes and gravity: a solid cell keeps them (SWEHR.c:721-803, 1233) */
     double *rain;
     double ds[SWEHR_MAX_CLASSES], pf[SWEHR_MAX_CLASSES];
     /* per-step scratch */
@@ -204,6 +215,48 @@ static void orc_neighbour(const orc_ctx *c, int i, int j, const double inflow[3]
     o->sstride = (size_t)c->N;
 }
 
+/* SOLID[i][j] as the reference reads it: inside the grid the mask; at
+ * j = ny+1 (the y-face test at SWEHR.c:1206,1211 reads one column past the
+ * row) the next row's first cell, SOLID[i+1][1], and past the last row 0 (the
+ * patched reference pads the matrix with zeros there); 0 elsewhere. */
+static int orc_solid(const orc_ctx *c, int i, int j)
+{
+    if (!c->solid || i < 1 || i > c->nx || j < 1) return 0;
+    if (j <= c->ny) return c->solid[IDX(c, i, j)] != 0;
+    if (j == c->ny + 1 && i < c->nx) return c->solid[IDX(c, i + 1, 1)] != 0;
+    return 0;
+}
+
+/* initialcondition's topography fill around solid cells (SWEHR.c:288-322),
+ * serial and in place, in the reference's order */
+static void orc_solid_fill(orc_ctx *c, double *T)
+{
+    const int nx = c->nx, ny = c->ny;
+#define S_(a, b) (c->solid[IDX(c, (a), (b))] != 0)
+#define T_(a, b) T[IDX(c, (a), (b))]
+    for (int i = 1; i <= nx; i++)
+        for (int j = 1; j <= ny; j++) {
+            int iup = i + 1 < nx ? i + 1 : nx, idown = i - 1 > 1 ? i - 1 : 1;
+            int jup = j + 1 < ny ? j + 1 : ny, jdown = j - 1 > 1 ? j - 1 : 1;
+            if (S_(i, j)) {
+                if (!S_(iup, j)) T_(i, j) = T_(iup, j);
+                if (!S_(idown, j)) T_(i, j) = T_(idown, j);
+                if (!S_(iup, jup)) T_(i, j) = T_(iup, jup);
+                if (!S_(iup, jdown)) T_(i, j) = T_(iup, jdown);
+                if (!S_(idown, jup)) T_(i, j) = T_(idown, jup);
+                if (!S_(idown, jdown)) T_(i, j) = T_(idown, jdown);
+                if (!S_(i, jup)) T_(i, j) = T_(i, jup);
+                if (!S_(i, jdown)) T_(i, j) = T_(i, jdown);
+            }
+            if (S_(iup, j) && !S_(i, j)) T_(iup, j) = T_(i, j);
+            if (S_(idown, j) && !S_(i, j)) T_(idown, j) = T_(i, j);
+            if (S_(i, jup) && !S_(i, j)) T_(i, jup) = T_(i, j);
+            if (S_(i, jdown) && !S_(i, j)) T_(i, jdown) = T_(i, j);
+        }
+#undef S_
+#undef T_
+}
+
 static double orc_nbsed(const orc_nb *o, int k)
 {
     return o->inflow ? o->sedin : o->sed[(size_t)k * o->sstride];
@@ -253,6 +306,11 @@ static int orc_step(orc_ctx *c)
             c->sxp[q] = sxp;
             c->syp[q] = syp;
             c->gzp[q] = g / M_POWH(sxp * sxp + syp * syp + 1);
+            if (c->solid && c->solid[q]) {         /* never recomputed (SWEHR.c:1233) */
+                c->sxn[q] = c->sxp[q] = c->sx0[q];
+                c->syn[q] = c->syp[q] = c->sy0[q];
+                c->gzp[q] = c->gz0[q];
+            }
         }
 
     /* phase 2: face fluxes and the largest wave speed (SWEHR.c:1092-1230) */
@@ -267,6 +325,11 @@ static int orc_step(orc_ctx *c)
                 orc_neighbour(c, i + 1, j, inflow, sedin, &Rn);
                 double gl = c->gzp[IDX(c, i == 0 ? 1 : i, j)];
                 double s = orc_hllc(L.h, Rn.h, L.hu, Rn.hu, L.hv, Rn.hv, gl, hfilm, T);
+                if (c->solid && i >= 1 && i < nx) {    /* reflecting faces, SWEHR.c:1137-1146 */
+                    int sl = orc_solid(c, i, j), sr = orc_solid(c, i + 1, j);
+                    if (sl && !sr) s = orc_hllc(Rn.h, Rn.h, -Rn.hu, Rn.hu, Rn.hv, Rn.hv, gl, hfilm, T);
+                    else if (!sl && sr) s = orc_hllc(L.h, L.h, L.hu, -L.hu, L.hv, L.hv, gl, hfilm, T);
+                }
                 double *f = c->fx + ((size_t)i * ny + (j - 1)) * NF;
                 f[0] = T[0]; f[1] = T[1]; f[2] = T[2];
                 for (int k = 0; k < S; k++)
@@ -278,6 +341,11 @@ static int orc_step(orc_ctx *c)
                 orc_neighbour(c, i, j + 1, inflow, sedin, &Rn);
                 double gl = c->gzp[IDX(c, i, j == 0 ? 1 : j)];
                 double s = orc_hllc(L.h, Rn.h, L.hv, Rn.hv, L.hu, Rn.hu, gl, hfilm, T);
+                if (c->solid && j >= 1) {              /* reflecting faces, SWEHR.c:1205-1214 */
+                    int sl = orc_solid(c, i, j), sr = orc_solid(c, i, j + 1);
+                    if (sl && !sr) s = orc_hllc(Rn.h, Rn.h, -Rn.hv, Rn.hv, Rn.hu, Rn.hu, gl, hfilm, T);
+                    else if (!sl && sr) s = orc_hllc(L.h, L.h, L.hv, -L.hv, L.hu, L.hu, gl, hfilm, T);
+                }
                 double *f = c->fy + ((size_t)(i - 1) * (ny + 1) + j) * NF;
                 f[0] = T[0]; f[1] = T[2]; f[2] = T[1];
                 for (int k = 0; k < S; k++)
@@ -293,6 +361,7 @@ static int orc_step(orc_ctx *c)
     for (int i = 1; i <= nx; i++)
         for (int j = 1; j <= ny; j++) {
             size_t q = IDX(c, i, j);
+            if (c->solid && c->solid[q]) continue;     /* no sources in a solid cell (SWEHR.c:1233) */
             double h = c->h[q], hu = c->hu[q], hv = c->hv[q];
             double rho = c->rho[q], totsed = c->totsed[q], totm = c->totm[q], dep = c->dep[q];
             double Rc = storm ? orc_storm(c, t, i, j) : R;
@@ -402,10 +471,30 @@ static int orc_step(orc_ctx *c)
     /* phase 4: cell update (SWEHR.c:1417-1588) */
     double b_out = 0, b_clamp = 0, b_bulk = 0, b_inf = 0, b_rain = 0;
     double b_det[SWEHR_MAX_CLASSES] = {0}, b_sout[SWEHR_MAX_CLASSES] = {0};
-#pragma omp parallel for schedule(static) reduction(+ : b_clamp, b_bulk, b_inf, b_rain, b_det[:SWEHR_MAX_CLASSES])
+    double b_solw = 0, b_sols[SWEHR_MAX_CLASSES] = {0};
+#pragma omp parallel for schedule(static) reduction(+ : b_clamp, b_bulk, b_inf, b_rain, b_solw, b_det[:SWEHR_MAX_CLASSES], b_sols[:SWEHR_MAX_CLASSES])
     for (int i = 1; i <= nx; i++)
         for (int j = 1; j <= ny; j++) {
             size_t q = IDX(c, i, j);
+            if (c->solid && c->solid[q]) {
+                /* outside the domain: no water, momentum or suspended sediment
+                 * (SWEHR.c:1566-1574); what a written state held there leaves
+                 * the budget as outflow */
+                b_solw += c->h[q];
+                c->h[q] = 0; c->hu[q] = 0; c->hv[q] = 0;
+                for (int k = 0; k < S; k++) {
+                    size_t qk = (size_t)k * N + q;
+                    b_sols[k] += c->U[qk];
+                    c->U[qk] = 0;
+                    c->sed[qk] = 0;
+                }
+                double rho = rhow * (1 - c->totsed[q]) + rhos * c->totsed[q];
+                if (rho > 0.8 * rhos) rho = 0.8 * rhos;
+                c->rho[q] = rho;
+                if (0.0 > c->maxvel[q]) c->maxvel[q] = 0.0;
+                if (0.0 > c->maxdep[q]) c->maxdep[q] = 0.0;
+                continue;
+            }
             const double *fxl = c->fx + ((size_t)(i - 1) * ny + (j - 1)) * NF;
             const double *fxr = c->fx + ((size_t)i * ny + (j - 1)) * NF;
             const double *fyl = c->fy + ((size_t)(i - 1) * (ny + 1) + (j - 1)) * NF;
@@ -525,6 +614,8 @@ static int orc_step(orc_ctx *c)
         b_out += dt * oneoverdx * (fr[0] - fl[0]);
         for (int k = 0; k < S; k++) b_sout[k] += dt * oneoverdx * (fr[3 + k] - fl[3 + k]);
     }
+    b_out += b_solw;
+    for (int k = 0; k < S; k++) b_sout[k] += b_sols[k];
     c->b_rain += b_rain; c->b_out += b_out; c->b_clamp += b_clamp; c->b_bulk += b_bulk; c->b_inf += b_inf;
     for (int k = 0; k < S; k++) { c->b_det[k] += b_det[k]; c->b_sout[k] += b_sout[k]; }
 
@@ -609,9 +700,26 @@ orc_ctx *orc_create(const swehr_params *p, const swehr_inputs *in)
         c->ks = (double *)orc_alloc(N);
         memcpy(c->ks, in->ks, N * sizeof(double));
     }
+    for (size_t q = 0; q < N; q++) c->z[q] = in->topo[q];
+    if (in->solid) {
+        c->solid = (int32_t *)calloc(N, sizeof(int32_t));
+        for (size_t q = 0; q < N; q++) c->solid[q] = in->solid[q] != 0;
+        orc_solid_fill(c, c->z);
+        c->sx0 = (double *)orc_alloc(N);
+        c->sy0 = (double *)orc_alloc(N);
+        c->gz0 = (double *)orc_alloc(N);
+        const double odx = 1 / p->dx;
+        for (int i = 1; i <= c->nx; i++)
+            for (int j = 1; j <= c->ny; j++) {
+                size_t q = IDX(c, i, j);
+                double sx = orc_slopex(c, c->z, i, j, odx), sy = orc_slopey(c, c->z, i, j, odx);
+                c->sx0[q] = sx;
+                c->sy0[q] = sy;
+                c->gz0[q] = p->g / M_POWH(sx * sx + sy * sy + 1);
+            }
+    }
     for (size_t q = 0; q < N; q++) {
-        c->z[q] = in->topo[q];
-        c->zp[q] = in->topo[q];
+        c->zp[q] = c->z[q];
         c->vinf[q] = p->vinf0;
         c->rho[q] = p->rhow * (1 - 0.0) + p->rhos * 0.0;   /* initialcondition, SWEHR.c:270 */
     }
@@ -629,8 +737,10 @@ void orc_destroy(orc_ctx *c)
     if (!c) return;
     double *bufs[] = {c->h, c->hu, c->hv, c->z, c->zp, c->vinf, c->maxvel, c->maxdep, c->totm, c->dep,
                       c->totsed, c->rho, c->sxn, c->syn, c->sxp, c->syp, c->gzp, c->U, c->M, c->sed,
-                      c->E, c->VF, c->srcf, c->fx, c->fy, c->rain, c->ks, c->stage, c->saveflow};
+                      c->E, c->VF, c->srcf, c->fx, c->fy, c->rain, c->ks, c->stage, c->saveflow,
+                      c->sx0, c->sy0, c->gz0};
     for (size_t f = 0; f < sizeof bufs / sizeof bufs[0]; f++) free(bufs[f]);
+    free(c->solid);
     free(c);
 }
 

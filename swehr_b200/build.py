@@ -67,8 +67,24 @@ def build(verbose: bool = False, ptxas_v: bool = False) -> str:
     if verbose:
         print(" ".join(cmd))
     subprocess.check_call(cmd)
+    build_probe(verbose)
     build_driver(verbose)
     return OUT
+
+
+PROBE = os.path.join(HERE, "libswehr_probe.so")
+
+
+def build_probe(verbose: bool = False) -> str:
+    """The benchmark's device-peak probe (FP64 pipe ceiling), its own library."""
+    src = os.path.join(CSRC, "swehr_probe.cu")
+    if os.path.exists(PROBE) and os.path.getmtime(PROBE) >= os.path.getmtime(src):
+        return PROBE
+    cmd = [nvcc()] + ARCH + ["-O3", "-std=c++17", "-Xcompiler", "-fPIC", "-shared", src, "-o", PROBE, "-lcudart"]
+    if verbose:
+        print(" ".join(cmd))
+    subprocess.check_call(cmd)
+    return PROBE
 
 
 DRIVER = os.path.join(HERE, "swehr_gpu")

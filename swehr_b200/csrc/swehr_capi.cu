@@ -105,10 +105,14 @@ static int64_t round_up(int64_t x, int64_t m) { return (x + m - 1) / m * m; }
  * control block, reduction partials and stage rows. */
 struct Layout {
     int64_t pitch, plane;
-    size_t rsize, set_bytes, off_z, off_ks, off_rain, off_ctl, off_partials, off_stage, off_saveflow, total;
+    size_t rsize, set_bytes, off_z, off_ks, off_solid, off_z0, off_rain, off_ctl, off_partials, off_stage,
+        off_saveflow, total;
 };
 
-static Layout layout_for(int nx, int ny, int S, int rnum, int has_ks, int64_t stagecap, int grid, int precision)
+/* ... with interior solid cells also the byte mask (one byte per plane
+ * element) and the set-up topography plane, after the Ks plane */
+static Layout layout_for(int nx, int ny, int S, int rnum, int has_ks, int has_solid, int64_t stagecap, int grid,
+                         int precision)
 {
     Layout L;
     L.pitch = round_up(ny, 32);
@@ -118,7 +122,9 @@ static Layout layout_for(int nx, int ny, int S, int rnum, int has_ks, int64_t st
     L.set_bytes = precision == SWEHR_MIXED ? (size_t)(9 + S) * pr + (size_t)(1 + S) * pb : (size_t)(P_FIXED + 2 * S) * pb;
     L.off_z = 2 * L.set_bytes;
     L.off_ks = L.off_z + 3 * pb;
-    L.off_rain = L.off_ks + (has_ks ? pr : 0);
+    L.off_solid = (size_t)round_up((int64_t)(L.off_ks + (has_ks ? pr : 0)), 256);
+    L.off_z0 = (size_t)round_up((int64_t)(L.off_solid + (has_solid ? (size_t)L.plane : 0)), 256);
+    L.off_rain = L.off_z0 + (has_solid ? pb : 0);
     L.off_ctl = (size_t)round_up((int64_t)(L.off_rain + (size_t)rnum * sizeof(double)), 256);
     L.off_partials = (size_t)round_up((int64_t)(L.off_ctl + sizeof(Ctl)), 256);
     L.off_stage = (size_t)round_up((int64_t)(L.off_partials + (size_t)grid * B_NTERMS * sizeof(double)), 256);
@@ -136,7 +142,7 @@ static int64_t stagecap_for(const swehr_params *p)
 
 extern "C" size_t swehr_footprint_bytes(int nx, int ny, int sclass, int precision)
 {
-    return layout_for(nx, ny, sclass, 64, 1, 4096, 148 * 4, precision).total;
+    return layout_for(nx, ny, sclass, 64, 1, 1, 4096, 148 * 4, precision).total;
 }
 
 static int validate(const swehr_params *p, const swehr_inputs *in)
@@ -153,6 +159,35 @@ static int validate(const swehr_params *p, const swehr_inputs *in)
     if (p->storm_peak > 0 && !(p->storm_radius > 0)) return set_err(SWEHR_INVALID, "storm_radius must be > 0");
     if (!in->topo || !in->rain || !in->ds || !in->pfrac) return set_err(SWEHR_INVALID, "NULL input array");
     return SWEHR_OK;
+}
+
+/* initialcondition's topography fill around interior solid cells
+ * (SWEHR.c:288-322): serial and in place, in the reference's order, so a
+ * cell filled early is read by later ones exactly as there.  T and solid
+ * are nx*ny, i-major. */
+static void solid_fill_topography(int nx, int ny, const int32_t *solid, std::vector<double> &T)
+{
+    auto S = [&](int i, int j) { return solid[(size_t)(i - 1) * ny + (j - 1)] != 0; };
+    auto Z = [&](int i, int j) -> double & { return T[(size_t)(i - 1) * ny + (j - 1)]; };
+    for (int i = 1; i <= nx; i++)
+        for (int j = 1; j <= ny; j++) {
+            const int iup = std::min(i + 1, nx), idown = std::max(i - 1, 1);
+            const int jup = std::min(j + 1, ny), jdown = std::max(j - 1, 1);
+            if (S(i, j)) {
+                if (!S(iup, j)) Z(i, j) = Z(iup, j);
+                if (!S(idown, j)) Z(i, j) = Z(idown, j);
+                if (!S(iup, jup)) Z(i, j) = Z(iup, jup);
+                if (!S(iup, jdown)) Z(i, j) = Z(iup, jdown);
+                if (!S(idown, jup)) Z(i, j) = Z(idown, jup);
+                if (!S(idown, jdown)) Z(i, j) = Z(idown, jdown);
+                if (!S(i, jup)) Z(i, j) = Z(i, jup);
+                if (!S(i, jdown)) Z(i, j) = Z(i, jdown);
+            }
+            if (S(iup, j) && !S(i, j)) Z(iup, j) = Z(i, j);
+            if (S(idown, j) && !S(i, j)) Z(idown, j) = Z(i, j);
+            if (S(i, jup) && !S(i, j)) Z(i, jup) = Z(i, j);
+            if (S(i, jdown) && !S(i, j)) Z(i, jdown) = Z(i, j);
+        }
 }
 
 template <class R>
@@ -179,6 +214,7 @@ static void make_devparams(const swehr_params *p, const swehr_inputs *in, const 
     P.outlet_row = p->outlet_row; P.npoints = p->npoints;
     for (int m = 0; m < 6; m++) { P.xpoint[m] = p->xpoint[m]; P.ypoint[m] = p->ypoint[m]; }
     P.has_ks = in->ks != nullptr;
+    P.has_solid = in->solid != nullptr;
     P.plane = L.plane;
     P.dx = p->dx; P.oneoverdx = 1 / p->dx; P.half_odx = 0.5 * P.oneoverdx; P.tend = p->tend; P.rint = p->rint;
     P.stageint = p->stageint;
@@ -354,7 +390,7 @@ static int download_plane(swehr_ctx *c, double *host, PlaneRef d, cudaStream_t s
 }
 
 template <class RS>
-static void set_views(BufsT<RS> &B, char *pool, const Layout &L, int S, int has_ks, int mixed)
+static void set_views(BufsT<RS> &B, char *pool, const Layout &L, int S, int has_ks, int has_solid, int mixed)
 {
     for (int s = 0; s < 2; s++) {
         char *base = pool + (size_t)s * L.set_bytes;
@@ -380,6 +416,8 @@ static void set_views(BufsT<RS> &B, char *pool, const Layout &L, int S, int has_
     }
     for (int k = 0; k < 3; k++) B.z[k] = (double *)(pool + L.off_z) + k * L.plane;
     B.ks = has_ks ? (const RS *)(pool + L.off_ks) : nullptr;
+    B.solid = has_solid ? (const uint8_t *)(pool + L.off_solid) : nullptr;
+    B.z0 = has_solid ? (const double *)(pool + L.off_z0) : nullptr;
 }
 
 /* a plane with v in its nx x ny cells and 0 in the row padding */
@@ -418,11 +456,11 @@ extern "C" int swehr_create(const swehr_params *p, const swehr_inputs *in, int p
     return swehr_ctx_create(p, in, precision, nullptr, out);
 }
 
-size_t swehr_ctx_footprint(const swehr_params *p, int has_ks, int precision, int num_sms)
+size_t swehr_ctx_footprint(const swehr_params *p, int has_ks, int has_solid, int precision, int num_sms)
 {
     /* num_sms 0: a pooled context (one reduction slot; pools sum with atomics) */
     const int grid = num_sms > 0 ? num_sms * 4 : 1;
-    return layout_for(p->nx, p->ny, p->sclass, p->rnum, has_ks, stagecap_for(p), grid, precision).total;
+    return layout_for(p->nx, p->ny, p->sclass, p->rnum, has_ks, has_solid, stagecap_for(p), grid, precision).total;
 }
 
 int swehr_ctx_create(const swehr_params *p, const swehr_inputs *in, int precision, const CtxHost *host,
@@ -456,7 +494,8 @@ int swehr_ctx_create(const swehr_params *p, const swehr_inputs *in, int precisio
     CKC(cudaDeviceGetAttribute(&c->num_sms, cudaDevAttrMultiProcessorCount, c->device));
     c->stagecap = stagecap_for(p);
     DevParams tmpP;
-    Layout L0 = layout_for(p->nx, p->ny, p->sclass, p->rnum, in->ks != nullptr, c->stagecap, 1, precision);
+    const int has_solid = in->solid != nullptr;
+    Layout L0 = layout_for(p->nx, p->ny, p->sclass, p->rnum, in->ks != nullptr, has_solid, c->stagecap, 1, precision);
     make_devparams(p, in, L0, tmpP);
     if (!pooled) {
         int ce = precision == SWEHR_MIXED ? configure_step_f32(tmpP, c->num_sms, c->cfg)
@@ -467,8 +506,8 @@ int swehr_ctx_create(const swehr_params *p, const swehr_inputs *in, int precisio
             return rc;
         }
     }
-    Layout L = layout_for(p->nx, p->ny, p->sclass, p->rnum, in->ks != nullptr, c->stagecap, c->cfg.grid_update,
-                          precision);
+    Layout L = layout_for(p->nx, p->ny, p->sclass, p->rnum, in->ks != nullptr, has_solid, c->stagecap,
+                          c->cfg.grid_update, precision);
     c->rsize = L.rsize;
     make_devparams(p, in, L, c->P);
     if (pooled) {
@@ -485,8 +524,8 @@ int swehr_ctx_create(const swehr_params *p, const swehr_inputs *in, int precisio
     }
     c->mem_bytes = L.total;
     CKC(cudaMemsetAsync(c->mem, 0, L.total, c->stream));
-    if (precision == SWEHR_MIXED) set_views(c->B32, c->mem, L, p->sclass, in->ks != nullptr, 1);
-    else set_views(c->B64, c->mem, L, p->sclass, in->ks != nullptr, 0);
+    if (precision == SWEHR_MIXED) set_views(c->B32, c->mem, L, p->sclass, in->ks != nullptr, has_solid, 1);
+    else set_views(c->B64, c->mem, L, p->sclass, in->ks != nullptr, has_solid, 0);
     c->d_rain = (double *)(c->mem + L.off_rain);
     c->d_ctl = (Ctl *)(c->mem + L.off_ctl);
     c->d_partials = (double *)(c->mem + L.off_partials);
@@ -511,8 +550,26 @@ int swehr_ctx_create(const swehr_params *p, const swehr_inputs *in, int precisio
     /* initial state (initialcondition, SWEHR.c:211-285): dry bed, VINF = vinf0, z = topo;
      * z of the previous step = z (setup slopes, SWEHR.c:721-803) */
     double *const *zpl = precision == SWEHR_MIXED ? c->B32.z : c->B64.z;
-    rc = upload_plane(c, PlaneRef{zpl[0], sizeof(double)}, in->topo, c->stream);
-    if (rc) { destroy_ctx(c); return rc; }
+    if (has_solid) {
+        /* the mask, and the topography filled around solid cells as
+         * initialcondition does (SWEHR.c:288-322); that filled topography is
+         * also the set-up plane solid cells' slopes come from */
+        const size_t N = (size_t)p->nx * p->ny;
+        std::vector<double> topo(in->topo, in->topo + N);
+        solid_fill_topography(p->nx, p->ny, in->solid, topo);
+        rc = upload_plane(c, PlaneRef{zpl[0], sizeof(double)}, topo.data(), c->stream);
+        if (rc) { destroy_ctx(c); return rc; }
+        std::vector<uint8_t> m(N);
+        for (size_t q = 0; q < N; q++) m[q] = in->solid[q] != 0;
+        CKC(cudaMemcpy2DAsync(c->mem + L.off_solid, (size_t)c->P.pitch, m.data(), (size_t)p->ny, (size_t)p->ny,
+                              (size_t)p->nx, cudaMemcpyHostToDevice, c->stream));
+        CKC(cudaMemcpyAsync(c->mem + L.off_z0, zpl[0], (size_t)c->P.plane * sizeof(double), cudaMemcpyDeviceToDevice,
+                            c->stream));
+        CKC(cudaStreamSynchronize(c->stream));      /* the host vectors go out of scope */
+    } else {
+        rc = upload_plane(c, PlaneRef{zpl[0], sizeof(double)}, in->topo, c->stream);
+        if (rc) { destroy_ctx(c); return rc; }
+    }
     for (int k = 1; k < 3; k++)     /* the other two z planes from the first, on the device */
         CKC(cudaMemcpyAsync(zpl[k], zpl[0], (size_t)c->P.plane * sizeof(double), cudaMemcpyDeviceToDevice, c->stream));
     rc = init_gz(c, 0);
@@ -811,6 +868,9 @@ extern "C" int swehr_write_field(swehr_ctx *c, int field, int k, const double *s
     if (field == SWEHR_FIELD_Z) {
         rc = upload_plane(c, z_plane(c, step), src, c->stream);
         if (!rc) rc = upload_plane(c, z_plane(c, step + 2), src, c->stream);
+        /* a written topography is a new set-up: solid cells take their slopes and GZ from it */
+        const double *z0 = c->precision == SWEHR_MIXED ? c->B32.z0 : c->B64.z0;
+        if (!rc && z0) rc = upload_plane(c, PlaneRef{const_cast<double *>(z0), sizeof(double)}, src, c->stream);
         if (!rc) rc = init_gz(c, step);
     } else {
         if ((field == SWEHR_FIELD_U || field == SWEHR_FIELD_M) && (k < 1 || k > c->P.S))

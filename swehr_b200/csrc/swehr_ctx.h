@@ -63,7 +63,7 @@ int swehr_ctx_create(const swehr_params *p, const swehr_inputs *in, int precisio
 
 /* device bytes swehr_ctx_create() allocates for these inputs (upper bound);
  * num_sms 0 for a pooled context */
-size_t swehr_ctx_footprint(const swehr_params *p, int has_ks, int precision, int num_sms);
+size_t swehr_ctx_footprint(const swehr_params *p, int has_ks, int has_solid, int precision, int num_sms);
 
 /* free a context (pools use this for their scenarios) */
 void swehr_ctx_destroy(swehr_ctx *c);

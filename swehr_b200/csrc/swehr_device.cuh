@@ -42,7 +42,7 @@ struct DevParams {
     int32_t rnum, inflow, storm, budget;
     int32_t bndry[4];
     int32_t outlet_row, npoints, xpoint[6], ypoint[6];
-    int32_t has_ks, pad_;
+    int32_t has_ks, has_solid;   /* per-cell Ks plane; interior solid mask (SOLID, SWEHR.c:597) */
     int64_t plane;        /* doubles per plane (>= nx*pitch, multiple of 32) */
     double dx, oneoverdx, half_odx, tend, rint, stageint;
     double g, hfilm, hfx10, rhos, rhow, rho0, porod, invporo;
@@ -151,6 +151,18 @@ __device__ __forceinline__ double hllc(double hl, double hr, double uhl, double 
     if (fabs(sr) > s) s = fabs(sr);
     if (fabs(sm) > s) s = fabs(sm);
     return s;
+}
+
+/* SOLID[i][j] as the reference's sweeps read it (m: the nx x pitch byte
+ * mask): inside the grid the mask; at j = ny+1 -- the y-face test at
+ * SWEHR.c:1206,1211 reads one column past the row -- the next row's first
+ * cell SOLID[i+1][1], and 0 past the last row; 0 elsewhere. */
+__device__ __forceinline__ bool solid_at(const DevParams &P, const uint8_t *__restrict__ m, int i, int j)
+{
+    if (i < 1 || i > P.nx || j < 1) return false;
+    if (j <= P.ny) return m[cidx(P, i, j)] != 0;
+    if (j == P.ny + 1 && i < P.nx) return m[cidx(P, i + 1, 1)] != 0;
+    return false;
 }
 
 /* SWEHR.c:1240-1257 */

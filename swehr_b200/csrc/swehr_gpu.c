@@ -186,7 +186,7 @@ int main(int argc, char **argv)
         }
     }
 
-    swehr_inputs inputs = {topo, rain, ds, pf, NULL};
+    swehr_inputs inputs = {topo, rain, ds, pf, NULL, NULL};
     swehr_ctx *ctx = NULL;
     check(swehr_create(&p, &inputs, precision, &ctx), "swehr_create");
 

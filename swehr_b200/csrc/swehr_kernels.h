@@ -16,12 +16,17 @@ struct SetV {
 };
 
 /* device buffers of one simulation: two state sets, the topography of the
- * previous, current and next step, optional per-cell Ks */
+ * previous, current and next step, optional per-cell Ks, and -- with
+ * interior solid cells -- the solid mask (one byte per cell, same pitch)
+ * and the topography at set-up, from which the slopes a solid cell keeps
+ * are taken (a solid cell never recomputes them, SWEHR.c:1233) */
 template <class RS>
 struct BufsT {
     SetV<RS> set[2];
     double *z[3];
     const RS *ks;
+    const uint8_t *solid;
+    const double *z0;
 };
 
 /* one scenario of a batch: everything its tiles need */

@@ -436,7 +436,7 @@ int swehr_pool_submit(swehr_pool *pl, const swehr_params *p, const swehr_inputs 
     if (p->budget && !pl->budget) return swehr_err(SWEHR_INVALID, "pool created without budgets");
     if (p->nx < 2 || p->ny < 2 || p->sclass < 1) return swehr_err(SWEHR_INVALID, "nx, ny >= 2 and sclass >= 1 required");
     /* admission by the largest block this scenario can occupy (grain, reuse slack) */
-    const size_t fp = swehr_ctx_footprint(p, in->ks != nullptr, pl->precision, 0);
+    const size_t fp = swehr_ctx_footprint(p, in->ks != nullptr, in->solid != nullptr, pl->precision, 0);
     const size_t want = (fp + kBlockGrain - 1) / kBlockGrain * kBlockGrain;
     const size_t bytes = want + want / 4;
     if (bytes > pl->hbm_limit) return swehr_err(SWEHR_INVALID, "scenario footprint exceeds the pool's HBM limit");

@@ -164,6 +164,16 @@ __device__ __forceinline__ typename PP::R hllc_v(typename PP::R hl, typename PP:
     return s;
 }
 
+/* The normal velocity of a state mirrored across a solid face: the
+ * reference negates the momentum and divides, (-hu)/h, when the side is wet
+ * (exactly -(hu/h), a zero included) and takes +0 when it is dry
+ * (SWEHR.c:333-352 on the arguments of SWEHR.c:1140,1145,1208,1213). */
+template <class PP>
+__device__ __forceinline__ typename PP::R mirror_v(typename PP::R vel, typename PP::R h, typename PP::R hfilm)
+{
+    return h > hfilm ? -vel : typename PP::R(0);
+}
+
 /* wave speed only (the same sl, sr, sm as hllc_v) */
 template <class PP>
 __device__ __forceinline__ typename PP::R hll_speed(typename PP::R hl, typename PP::R hr, typename PP::R nl,
@@ -373,7 +383,7 @@ __device__ __forceinline__ double sslope_y(const DevParams &P, const double *zs,
  * dry), GZ of the previous step and sqrt(GZ h) for left/lower face cells,
  * SED_k.  Ghost cells read their source cell (SWEHR.c:816-1035). */
 template <class PP, class RS>
-__device__ __forceinline__ void stage_derive(const DevParams &P, TileCoord tc, unsigned char *smb,
+__device__ __forceinline__ void stage_derive(const DevParams &P, const SetV<RS> &src, TileCoord tc, unsigned char *smb,
                                              const StagedLayout &L, typename PP::R inh, typename PP::R inhv,
                                              typename PP::R insed)
 {
@@ -414,10 +424,17 @@ __device__ __forceinline__ void stage_derive(const DevParams &P, TileCoord tc, u
         su[idx] = u;
         sv[idx] = v;
         if (hi <= T_I && hj <= T_J) {
-            /* GZ of the previous step at the source cell, SWEHR.c:1279 via z_prev */
-            const int zr = si - (tc.i0 - 2);
-            const R sx = (R)sslope_x(P, zps, zr, scol, si), sy = (R)sslope_y(P, zps, zr, scol, sj);
-            const R g = PP::div(K.g, PP::sqrtp(sx * sx + sy * sy + 1));
+            R g;
+            if (P.has_solid) {
+                /* the state's GZ plane: the previous step's GZ of a flow cell,
+                 * the set-up GZ a solid cell keeps (SWEHR.c:1233) */
+                g = (R)src.gz[cidx(P, si, sj)];
+            } else {
+                /* GZ of the previous step at the source cell, SWEHR.c:1279 via z_prev */
+                const int zr = si - (tc.i0 - 2);
+                const R sx = (R)sslope_x(P, zps, zr, scol, si), sy = (R)sslope_y(P, zps, zr, scol, sj);
+                g = PP::div(K.g, PP::sqrtp(sx * sx + sy * sy + 1));
+            }
             sg[idx] = g;
             sc[idx] = PP::sqrtp(g * h);
         }
@@ -468,10 +485,16 @@ __device__ __forceinline__ typename PP::R lagged_gz(const DevParams &P, const do
     return PP::div(K.g, PP::sqrtp(sx * sx + sy * sy + 1));
 }
 
-/* wave_cell with the cell's lagged GZ given (g) */
+/* wave_cell with the cell's lagged GZ given (g).  solid: the interior
+ * solid mask, or nullptr; a face between a solid and a flow cell takes the
+ * flow cell's state mirrored across it (SWEHR.c:1137-1146 for i+1/2 with
+ * 1 <= i < nx, 1205-1214 for j+1/2, the latter reading the mask one column
+ * past the row at j = ny, see solid_at), with the GZ of the face's left
+ * (lower) cell as every face does. */
 template <class PP, class RS>
 __device__ __forceinline__ typename PP::R wave_cell_g(const DevParams &P, const SetV<RS> &src, int i, int j,
-                                                      typename PP::R inh, typename PP::R inhv, typename PP::R g)
+                                                      typename PP::R inh, typename PP::R inhv, typename PP::R g,
+                                                      const uint8_t *__restrict__ solid = nullptr)
 {
     typedef typename PP::R R;
     const RealC<R> &K = kc<R>(P);
@@ -483,29 +506,42 @@ __device__ __forceinline__ typename PP::R wave_cell_g(const DevParams &P, const 
         v = PP::div(hv, h);
     }
     const R c = PP::sqrtp(g * h);
+    const bool here_solid = solid && solid_at(P, solid, i, j);
     R smax = 0, s;
     /* x face i+1/2 */
     if (i < P.nx) {
         const int64_t qr = q + P.pitch;
         const R hr = (R)src.h[qr];
         const R ur = hr > K.hfilm ? PP::div((R)src.hu[qr], hr) : R(0);
-        s = hll_speed<PP>(h, hr, u, ur, g, c, K.hfilm);
+        const bool right_solid = solid && solid_at(P, solid, i + 1, j);
+        if (here_solid && !right_solid)
+            s = hll_speed<PP>(hr, hr, mirror_v<PP>(ur, hr, K.hfilm), ur, g, PP::sqrtp(g * hr), K.hfilm);
+        else if (!here_solid && right_solid) s = hll_speed<PP>(h, h, u, mirror_v<PP>(u, h, K.hfilm), g, c, K.hfilm);
+        else s = hll_speed<PP>(h, hr, u, ur, g, c, K.hfilm);
     } else {
         s = hll_speed<PP>(h, h, u, P.bndry[2] == 1 ? -u : u, g, c, K.hfilm);
     }
     smax = (s > smax) ? s : smax;
-    /* y face j+1/2 */
-    if (j < P.ny) {
-        const int64_t qr = q + 1;
-        const R hr = (R)src.h[qr];
-        const R vr = hr > K.hfilm ? PP::div((R)src.hv[qr], hr) : R(0);
-        s = hll_speed<PP>(h, hr, v, vr, g, c, K.hfilm);
-    } else if (P.inflow) {
-        const R hr = (R)(RS)inh;             /* the ghost's depth as the tile pass staged it */
-        const R vr = inh > K.hfilm ? PP::div(inhv, inh) : R(0);
-        s = hll_speed<PP>(h, hr, v, vr, g, c, K.hfilm);
-    } else {
-        s = hll_speed<PP>(h, h, v, P.bndry[3] == 1 ? -v : v, g, c, K.hfilm);
+    /* y face j+1/2: the right state is cell (i, j+1), or at j = ny the ghost
+     * (the inflow ramp, or this cell with its normal velocity negated at a wall) */
+    {
+        R hr, vr;
+        if (j < P.ny) {
+            const int64_t qr = q + 1;
+            hr = (R)src.h[qr];
+            vr = hr > K.hfilm ? PP::div((R)src.hv[qr], hr) : R(0);
+        } else if (P.inflow) {
+            hr = (R)(RS)inh;                     /* the ghost's depth as the tile pass staged it */
+            vr = inh > K.hfilm ? PP::div(inhv, inh) : R(0);
+        } else {
+            hr = h;
+            vr = P.bndry[3] == 1 ? -v : v;
+        }
+        const bool right_solid = solid && solid_at(P, solid, i, j + 1);
+        if (here_solid && !right_solid)
+            s = hll_speed<PP>(hr, hr, mirror_v<PP>(vr, hr, K.hfilm), vr, g, PP::sqrtp(g * hr), K.hfilm);
+        else if (!here_solid && right_solid) s = hll_speed<PP>(h, h, v, mirror_v<PP>(v, h, K.hfilm), g, c, K.hfilm);
+        else s = hll_speed<PP>(h, hr, v, vr, g, c, K.hfilm);
     }
     smax = (s > smax) ? s : smax;
     /* the domain's faces 1/2: ghost on the left, this cell on the right */
@@ -522,10 +558,11 @@ __device__ __forceinline__ typename PP::R wave_cell_g(const DevParams &P, const 
 
 template <class PP, class RS>
 __device__ __forceinline__ typename PP::R wave_cell(const DevParams &P, const SetV<RS> &src, int i, int j,
-                                                    typename PP::R inh, typename PP::R inhv)
+                                                    typename PP::R inh, typename PP::R inhv,
+                                                    const uint8_t *__restrict__ solid)
 {
     /* GZ of the previous step, written by its update */
-    return wave_cell_g<PP, RS>(P, src, i, j, inh, inhv, (typename PP::R)src.gz[cidx(P, i, j)]);
+    return wave_cell_g<PP, RS>(P, src, i, j, inh, inhv, (typename PP::R)src.gz[cidx(P, i, j)], solid);
 }
 
 /* block maximum of the threads' partial maxima (result valid in thread 0) */
@@ -579,7 +616,7 @@ __global__ void __launch_bounds__(TILE_THREADS, PP::kWaveMinBlocks) k_wave_cells
     int i = (int)(c0 / P.ny) + 1, j = (int)(c0 - (int64_t)(i - 1) * P.ny) + 1;
     R smax = 0;
     for (int64_t c = c0; c < total; c += stride) {
-        const R s = wave_cell<PP, RS>(P, src, i, j, (R)inh, (R)inhv);
+        const R s = wave_cell<PP, RS>(P, src, i, j, (R)inh, (R)inhv, P.has_solid ? B.solid : nullptr);
         smax = (s > smax) ? s : smax;
         i += si;
         j += sj;
@@ -622,6 +659,8 @@ struct FailArgs {
     int32_t nx, ny, pitch, pad_;
     int64_t plane;
     double oneoverdx, half_odx, rho0, rhow, cohesion, fa;
+    const uint8_t *solid;      /* interior solid mask or nullptr */
+    const double *z0;          /* set-up topography: a solid neighbour's slopes */
 };
 
 __device__ __forceinline__ double fa_slope_x(const FailArgs &A, const double *__restrict__ z, int i, int j)
@@ -653,10 +692,14 @@ __device__ __noinline__ typename PP::R fail_exact(const FailArgs A, const RS *__
     typedef typename PP::R R;
     const int iu = (i < A.nx) ? i + 1 : A.nx, id = (i > 1) ? i - 1 : 1;
     const int ju = (j < A.ny) ? j + 1 : A.ny, jd = (j > 1) ? j - 1 : 1;
-    const R sxu = (iu == i) ? sx : (R)fa_slope_x(A, zp, iu, j);
-    const R sxd = (id == i) ? sx : (R)fa_slope_x(A, zc, id, j);
-    const R syu = (ju == j) ? sy : (R)fa_slope_y(A, zp, i, ju);
-    const R syd = (jd == j) ? sy : (R)fa_slope_y(A, zc, i, jd);
+    /* a solid neighbour never recomputed its slopes (SWEHR.c:1233): they are the set-up ones */
+    auto zfor = [&](int ii, int jj, const double *z) {
+        return (A.solid && A.solid[(int64_t)(ii - 1) * A.pitch + (jj - 1)]) ? A.z0 : z;
+    };
+    const R sxu = (iu == i) ? sx : (R)fa_slope_x(A, zfor(iu, j, zp), iu, j);
+    const R sxd = (id == i) ? sx : (R)fa_slope_x(A, zfor(id, j, zc), id, j);
+    const R syu = (ju == j) ? sy : (R)fa_slope_y(A, zfor(i, ju, zp), i, ju);
+    const R syd = (jd == j) ? sy : (R)fa_slope_y(A, zfor(i, jd, zc), i, jd);
     const R rho0 = (R)A.rho0, half = R(0.5), odx = (R)A.oneoverdx;
     auto D = [&](int ii, int jj) { return (R)dep_plane[(int64_t)(ii - 1) * A.pitch + (jj - 1)]; };
     R fail = 0;
@@ -686,11 +729,44 @@ __device__ __forceinline__ typename PP::R storm_r(const DevParams &P, double t, 
     return (R)P.storm_peak * PP::exp(R(-0.5 * r2));
 }
 
+/* A solid cell in the update (SWEHR.c:1421 false branch, 1566-1574): no
+ * water, momentum or suspended sediment; everything else -- deposit,
+ * infiltration, topography, maxima, its GZ -- as it was.  What a written
+ * state held there leaves the budget as outflow. */
+template <class PP, class RS, int MAXS, bool BUDGET>
+__device__ __noinline__ void solid_cell(const DevParams &P, const SetV<RS> &src, const SetV<RS> &dst,
+                                        const double *__restrict__ zc, double *__restrict__ zn, int64_t q,
+                                        Acc2<MAXS, BUDGET> &acc)
+{
+    const int64_t pl = P.plane;
+    if (BUDGET) acc.out += (double)src.h[q];
+    dst.h[q] = (RS)0;
+    dst.hu[q] = (RS)0;
+    dst.hv[q] = (RS)0;
+    for (int k = 0; k < P.S; k++) {
+        if (BUDGET && k < MAXS) acc.sout[k] += (double)src.U[k * pl + q];
+        dst.U[k * pl + q] = (RS)0;
+        dst.M[k * pl + q] = src.M[k * pl + q];
+    }
+    dst.vinf[q] = src.vinf[q];
+    RS mv = src.maxvel[q], md = src.maxdep[q];
+    if ((RS)0 > mv) mv = (RS)0;
+    if ((RS)0 > md) md = (RS)0;
+    dst.maxvel[q] = mv;
+    dst.maxdep[q] = md;
+    dst.totm[q] = src.totm[q];
+    dst.dep[q] = src.dep[q];
+    dst.totsed[q] = src.totsed[q];
+    dst.gz[q] = src.gz[q];
+    zn[q] = zc[q];
+}
+
 template <class PP, class RS, int MAXS, bool BUDGET>
 __device__ __forceinline__ void tile_cell(const DevParams &P, const SetV<RS> &src, const SetV<RS> &dst,
                                           const double *__restrict__ zp, const double *__restrict__ zc,
                                           double *__restrict__ zn, const unsigned char *smb, const StagedLayout &L,
-                                          TileCoord tc, double t, double dt, double Rr, Acc2<MAXS, BUDGET> &acc)
+                                          TileCoord tc, double t, double dt, double Rr, Acc2<MAXS, BUDGET> &acc,
+                                          const uint8_t *__restrict__ solid, const double *__restrict__ z0)
 {
     typedef typename PP::R R;
     const RealC<R> &K = kc<R>(P);
@@ -699,6 +775,10 @@ __device__ __forceinline__ void tile_cell(const DevParams &P, const SetV<RS> &sr
     if (i > P.nx || j > P.ny) return;
     const int64_t pl = P.plane;
     const int64_t q = cidx(P, i, j);
+    if (P.has_solid && solid[q]) {
+        solid_cell<PP, RS, MAXS, BUDGET>(P, src, dst, zc, zn, q, acc);
+        return;
+    }
     const int S = P.S;
     const R hfilm = K.hfilm, rhos = K.rhos, rhow = K.rhow, one = 1, half = R(0.5);
     const int hs = (ti + 1) * H_J + (tj + 1);                      /* this cell in halo coords */
@@ -769,6 +849,7 @@ __device__ __forceinline__ void tile_cell(const DevParams &P, const SetV<RS> &sr
             fa.nx = P.nx; fa.ny = P.ny; fa.pitch = P.pitch; fa.pad_ = 0; fa.plane = P.plane;
             fa.oneoverdx = P.oneoverdx; fa.half_odx = P.half_odx; fa.rho0 = P.rho0; fa.rhow = P.rhow;
             fa.cohesion = P.cohesion; fa.fa = P.fa;
+            fa.solid = P.has_solid ? solid : nullptr; fa.z0 = z0;
             fail = fail_exact<PP, RS>(fa, src.dep, zp, zc, i, j, sx, sy, gz, dep0, rho0c, h0v);
         }
     }
@@ -1073,7 +1154,7 @@ __device__ __forceinline__ void update_tile(const DevParams &P, const BufsT<RS> 
     stage_load<RS>(P, src, zp, zc, B.ks, tc, smb, L);
     __pipeline_wait_prior(0);
     __syncthreads();
-    stage_derive<PP, RS>(P, tc, smb, L, (R)inh, (R)inhv, (R)insed);
+    stage_derive<PP, RS>(P, src, tc, smb, L, (R)inh, (R)inhv, (R)insed);
     __syncthreads();
     const RS *sh = staged_h<RS>(smb, L);
     /* stage B: every face of the tile (SWEHR.c:1099-1230) */
@@ -1084,8 +1165,22 @@ __device__ __forceinline__ void update_tile(const DevParams &P, const BufsT<RS> 
             const int gi = tc.i0 - 1 + fi, gj = tc.j0 + fj;
             if (gj > P.ny || gi > P.nx) continue;
             const int Lh = fi * H_J + fj + 1, Rh = Lh + H_J;
-            hllc_v<PP>((R)sh[fi * R_J + fj + 2], (R)sh[(fi + 1) * R_J + fj + 2], su[Lh], su[Rh], sv[Lh], sv[Rh],
-                       sg[Lh], sc[Lh], K.hfilm, T0, T1, T2);
+            const R hl = (R)sh[fi * R_J + fj + 2], hr = (R)sh[(fi + 1) * R_J + fj + 2];
+            int var = 0;                 /* 1: solid left, 2: solid right (SWEHR.c:1137-1146) */
+            if (P.has_solid && gi >= 1 && gi < P.nx) {
+                const bool sl = solid_at(P, B.solid, gi, gj), sr = solid_at(P, B.solid, gi + 1, gj);
+                var = (sl && !sr) ? 1 : ((!sl && sr) ? 2 : 0);
+            }
+            /* the mirrored normal velocity is (-hu)/h when wet (a zero keeps its
+             * negated sign, as in the reference) and +0 when dry */
+            if (var == 1)
+                hllc_v<PP>(hr, hr, mirror_v<PP>(su[Rh], hr, K.hfilm), su[Rh], sv[Rh], sv[Rh], sg[Lh],
+                           PP::sqrtp(sg[Lh] * hr), K.hfilm, T0, T1, T2);
+            else if (var == 2)
+                hllc_v<PP>(hl, hl, su[Lh], mirror_v<PP>(su[Lh], hl, K.hfilm), sv[Lh], sv[Lh], sg[Lh], sc[Lh], K.hfilm,
+                           T0, T1, T2);
+            else
+                hllc_v<PP>(hl, hr, su[Lh], su[Rh], sv[Lh], sv[Rh], sg[Lh], sc[Lh], K.hfilm, T0, T1, T2);
             R *F = sfx + 3 * f;
             F[0] = T0; F[1] = T1; F[2] = T2;
             upb[f] = (T0 > 0) ? 0 : 1;
@@ -1095,15 +1190,27 @@ __device__ __forceinline__ void update_tile(const DevParams &P, const BufsT<RS> 
             const int gi = tc.i0 + fi, gj = tc.j0 - 1 + fj;
             if (gi > P.nx || gj > P.ny) continue;
             const int Lh = (fi + 1) * H_J + fj, Rh = Lh + 1;
-            hllc_v<PP>((R)sh[(fi + 1) * R_J + fj + 1], (R)sh[(fi + 1) * R_J + fj + 2], sv[Lh], sv[Rh], su[Lh],
-                       su[Rh], sg[Lh], sc[Lh], K.hfilm, T0, T1, T2);
+            const R hl = (R)sh[(fi + 1) * R_J + fj + 1], hr = (R)sh[(fi + 1) * R_J + fj + 2];
+            int var = 0;                 /* 1: solid below, 2: solid above (SWEHR.c:1205-1214) */
+            if (P.has_solid && gj >= 1) {
+                const bool sl = solid_at(P, B.solid, gi, gj), sr = solid_at(P, B.solid, gi, gj + 1);
+                var = (sl && !sr) ? 1 : ((!sl && sr) ? 2 : 0);
+            }
+            if (var == 1)
+                hllc_v<PP>(hr, hr, mirror_v<PP>(sv[Rh], hr, K.hfilm), sv[Rh], su[Rh], su[Rh], sg[Lh],
+                           PP::sqrtp(sg[Lh] * hr), K.hfilm, T0, T1, T2);
+            else if (var == 2)
+                hllc_v<PP>(hl, hl, sv[Lh], mirror_v<PP>(sv[Lh], hl, K.hfilm), su[Lh], su[Lh], sg[Lh], sc[Lh], K.hfilm,
+                           T0, T1, T2);
+            else
+                hllc_v<PP>(hl, hr, sv[Lh], sv[Rh], su[Lh], su[Rh], sg[Lh], sc[Lh], K.hfilm, T0, T1, T2);
             R *F = sfy + 3 * f2;
             F[0] = T0; F[1] = T2; F[2] = T1;
             upb[f] = (T0 > 0) ? 0 : 1;
         }
     }
     __syncthreads();
-    tile_cell<PP, RS, MAXS, BUDGET>(P, src, dst, zp, zc, zn, smb, L, tc, t, dt, Rr, acc);
+    tile_cell<PP, RS, MAXS, BUDGET>(P, src, dst, zp, zc, zn, smb, L, tc, t, dt, Rr, acc, B.solid, B.z0);
     __syncthreads();
 }
 
@@ -1351,7 +1458,8 @@ __global__ void __launch_bounds__(TILE_THREADS) k_wave_batch(const BatchHdr<RS> 
             const TileCoord tc = tile_coord(sd.P, g - sd.tile0);
             const int i = tc.i0 + (int)threadIdx.x / T_J, j = tc.j0 + (int)threadIdx.x % T_J;
             if (i <= sd.P.nx && j <= sd.P.ny) {
-                const R s = wave_cell<PP, RS>(sd.P, sd.B.set[n & 1], i, j, (R)snap_inh, (R)snap_inhv);
+                const R s = wave_cell<PP, RS>(sd.P, sd.B.set[n & 1], i, j, (R)snap_inh, (R)snap_inhv,
+                                              sd.P.has_solid ? sd.B.solid : nullptr);
                 smax = (s > smax) ? s : smax;
             }
             run++;

@@ -98,12 +98,17 @@ class CaseInputs:
         self._ds = np.ascontiguousarray(case.ds, dtype=np.float64)
         self._pf = np.ascontiguousarray(case.pfrac, dtype=np.float64)
         self._ks = None if case.ks is None else np.ascontiguousarray(case.ks, dtype=np.float64)
+        solid = getattr(case, "solid", None)
+        self._solid = None if solid is None else np.ascontiguousarray(solid, dtype=np.int32)
         self.inputs = SwehrInputs(_dptr(self._topo), _dptr(self._rain), _dptr(self._ds), _dptr(self._pf),
-                                  _dptr(self._ks) if self._ks is not None else None)
+                                  _dptr(self._ks) if self._ks is not None else None,
+                                  self._solid.ctypes.data_as(C.POINTER(C.c_int32)) if self._solid is not None
+                                  else None)
 
     @property
     def host_bytes(self) -> int:
         n = self._topo.nbytes + self._rain.nbytes + self._ds.nbytes + self._pf.nbytes
+        n += self._solid.nbytes if self._solid is not None else 0
         return n + (self._ks.nbytes if self._ks is not None else 0)
 
 

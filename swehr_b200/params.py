@@ -53,7 +53,7 @@ class SwehrInputs(C.Structure):
     _fields_ = [
         ("topo", C.POINTER(C.c_double)), ("rain", C.POINTER(C.c_double)),
         ("ds", C.POINTER(C.c_double)), ("pfrac", C.POINTER(C.c_double)),
-        ("ks", C.POINTER(C.c_double)),
+        ("ks", C.POINTER(C.c_double)), ("solid", C.POINTER(C.c_int32)),
     ]
 
 

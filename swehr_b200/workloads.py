@@ -15,6 +15,10 @@ text files written by swehr_b200.io) and the GPU read identical bits.
   failure_tiny(), failure_hillslope()
                      cross-sloped grids with the deposit cohesion lowered,
                      so the slope-failure branch fires
+  solid_tiny(), solid_hillslope()
+                     grids with interior solid cells (blocks, a wall, a
+                     cell in the first column whose mask the last column's
+                     y-face test reads)
 """
 from __future__ import annotations
 
@@ -39,6 +43,7 @@ class Case:
     pfrac: np.ndarray                 # (S,)
     ks: Optional[np.ndarray] = None   # (nx, ny) m/s or None
     max_steps: int = -1               # -1: run to tend
+    solid: Optional[np.ndarray] = None  # (nx, ny) int32 interior solid mask or None
 
     @property
     def nx(self):
@@ -219,4 +224,35 @@ def failure_hillslope(cross: float = 0.4, cohesion: float = 20.0, tend: float = 
     c.params["cohesion"] = cohesion
     c.params["tend"] = tend
     c.name = "failure_hillslope200x50"
+    return c
+
+
+def solid_tiny(nx: int = 20, ny: int = 16, S: int = 4, seed: int = 51, **kw) -> Case:
+    """tiny_case with interior solid cells: a 4x4 block, a one-cell-wide wall
+    with a gap, and the cell (3, 1) -- the reference's y-face test at j = ny
+    reads SOLID[i][ny+1], which is SOLID[i+1][1] (SWEHR.c:1206,1211), so
+    cell (2, ny) gets a reflecting top face from it."""
+    c = tiny_case(nx=nx, ny=ny, S=S, seed=seed, **kw)
+    m = np.zeros((nx, ny), dtype=np.int32)
+    m[5:9, 4:8] = 1
+    m[12, 2:ny - 3] = 1
+    m[12, ny // 2] = 0
+    m[2, 0] = 1
+    c.solid = m
+    c.name = f"solid{nx}x{ny}s{S}"
+    return c
+
+
+def solid_hillslope(tend: float = 600.0) -> Case:
+    """The 200x50 hillslope with three rectangular buildings and a wall
+    across part of the slope, run to `tend`."""
+    c = hillslope200x50()
+    m = np.zeros((c.nx, c.ny), dtype=np.int32)
+    m[40:52, 10:18] = 1
+    m[90:96, 30:44] = 1
+    m[150:170, 5:9] = 1
+    m[120, 0:35] = 1
+    c.solid = m
+    c.params["tend"] = tend
+    c.name = "solid_hillslope200x50"
     return c

@@ -15,6 +15,10 @@ oracle/build_ref.py, on:
   failure_*.npz     cross-sloped grids with the deposit cohesion lowered
                     (two small ones and the 200x50 hillslope to 600 s):
                     slope failure fires (SWEHR.c:1292-1312, 1497-1503)
+  solid_*.npz       interior solid cells (two small grids and the 200x50
+                    hillslope with buildings and a wall, to 600 s): the
+                    topography fill, reflecting faces and the source skip
+                    (SWEHR.c:288-322, 1137-1146, 1205-1214, 1233)
   shipped_files.npz the reference's own output files for the shipped
                     example run as shipped (movies on): the ten result
                     grids, stage.txt, saveflow.txt, every 30th frame of the
@@ -56,6 +60,11 @@ FAILURE = [
     dict(slope_y=0.7, cohesion=50.0, nx=17, ny=13, S=7, seed=32, bndry=(1, 1, 0, 0), rain_mmh=200.0, tend=150.0),
 ]
 
+SOLID = [
+    dict(bndry=(1, 1, 1, 1), inflow=1, S=3, seed=52),
+    dict(bndry=(0, 0, 0, 0), rain_mmh=500.0, seed=53),
+]
+
 DUMP_KEYS = ("h", "hu", "hv", "z", "vinf", "totm", "dep", "totsed", "maxvel", "maxdepth", "U", "M", "sed",
              "stage", "saveflow")
 
@@ -65,6 +74,8 @@ def save(path, case, dumps: dict):
             "ds": case.ds, "pfrac": case.pfrac, "name": np.array(case.name)}
     if case.ks is not None:
         arrs["ks"] = case.ks
+    if getattr(case, "solid", None) is not None:
+        arrs["solid"] = case.solid
     for tag, d in dumps.items():
         arrs[f"{tag}__steps"] = np.array(d["steps"])
         arrs[f"{tag}__t"] = np.array(d["t"])
@@ -142,10 +153,22 @@ def failure_fixtures():
     save(os.path.join(HERE, "failure_hillslope.npz"), c, {"end": d})
 
 
+def solid_fixtures():
+    for n, kw in enumerate(SOLID):
+        c = W.solid_tiny(**kw)
+        c.params["bndry"] = list(c.params["bndry"])
+        d, _ = harness.run_reference(c)
+        save(os.path.join(HERE, f"solid_{n}.npz"), c, {"end": d})
+    c = W.solid_hillslope()
+    c.params["bndry"] = list(c.params["bndry"])
+    d, _ = harness.run_reference(c)
+    save(os.path.join(HERE, "solid_hillslope.npz"), c, {"end": d})
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--reference", default=None, help="reference checkout (default: $SWEHR_REFERENCE)")
-    ap.add_argument("--only", default=None, help="shipped_files | failure: only regenerate those fixtures")
+    ap.add_argument("--only", default=None, help="shipped_files | failure | solid: only regenerate those fixtures")
     a = ap.parse_args()
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import build_ref
@@ -158,6 +181,10 @@ def main():
     if a.only in (None, "failure"):
         failure_fixtures()
         if a.only == "failure":
+            return
+    if a.only in (None, "solid"):
+        solid_fixtures()
+        if a.only == "solid":
             return
     c = shipped_case(a.reference)
     d1, _ = harness.run_reference(c, max_steps=2000)

@@ -43,8 +43,11 @@ class _Inputs:
         self.ds = np.ascontiguousarray(case.ds, dtype=np.float64)
         self.pf = np.ascontiguousarray(case.pfrac, dtype=np.float64)
         self.ks = None if case.ks is None else np.ascontiguousarray(case.ks, dtype=np.float64)
+        solid = getattr(case, "solid", None)
+        self.solid = None if solid is None else np.ascontiguousarray(solid, dtype=np.int32)
         self.s = SwehrInputs(_dptr(self.topo), _dptr(self.rain), _dptr(self.ds), _dptr(self.pf),
-                             _dptr(self.ks) if self.ks is not None else None)
+                             _dptr(self.ks) if self.ks is not None else None,
+                             self.solid.ctypes.data_as(C.POINTER(C.c_int32)) if self.solid is not None else None)
 
 
 class OracleRun:
@@ -208,7 +211,7 @@ def load_golden(name: str):
     if "bndry" in params:
         params["bndry"] = tuple(params["bndry"])
     case = Case(str(z["name"]), params, z["topo"], z["rain"], z["ds"], z["pfrac"],
-                ks=z["ks"] if "ks" in z.files else None)
+                ks=z["ks"] if "ks" in z.files else None, solid=z["solid"] if "solid" in z.files else None)
     dumps = {}
     for key in z.files:
         if "__" in key:

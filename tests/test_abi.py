@@ -43,7 +43,7 @@ def test_library_exports_every_declared_symbol():
 def test_params_struct_and_defaults_match_reference():
     L = swlib.load()
     assert L.swehr_params_size() == C.sizeof(SwehrParams)
-    assert L.swehr_abi_version() == 1
+    assert L.swehr_abi_version() == 2
     p = SwehrParams()
     L.swehr_params_default(C.byref(p))
     d = params_dict(p)

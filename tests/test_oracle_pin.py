@@ -60,6 +60,24 @@ def test_glibc_oracle_matches_reference_slope_failure(name):
     assert np.array_equal(st, d["stage"], equal_nan=True)
 
 
+@pytest.mark.parametrize("name", ["solid_0", "solid_1", "solid_hillslope"])
+def test_glibc_oracle_matches_reference_solid_cells(name):
+    """Interior solid cells (a SOLID mask the patched reference reads from
+    solid.txt): the topography fill (SWEHR.c:288-322), reflecting faces
+    (SWEHR.c:1137-1146, 1205-1214, including the y-face test's read of the
+    next row's first cell at j = ny) and the source skip (SWEHR.c:1233)."""
+    case, dumps = load_golden(name)
+    assert case.solid is not None and case.solid.any()
+    o = OracleRun(case, "glibc")
+    o.advance()
+    d = dumps["end"]
+    assert o.steps == d["steps"] and o.t == d["t"]
+    f = o.fields()
+    assert not _bitexact(f, d)
+    m = case.solid.astype(bool)
+    assert (f["h"][m] == 0).all() and (f["U"][:, m] == 0).all()
+
+
 def test_glibc_oracle_matches_reference_shipped_example():
     case, dumps = load_golden("shipped")
     o = OracleRun(case, "glibc")
