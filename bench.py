@@ -209,7 +209,7 @@ def ensemble_leg(args, ranks):
     mine = shard([c.cells() for c in all_cases], ranks.world)[ranks.rank]
     cases = [all_cases[k] for k in mine]
     cells = sum(c.cells() for c in all_cases)
-    cap = 64 + args.ens_warmup + args.ens_steps
+    cap = 64 + args.ens_warmup + args.ens_steps   # pool steps every scenario runs (the tuner's included)
     every = max(1, len(all_cases) // 8)
     subset = [i for i, k in enumerate(mine) if k % every == 0 and k // every < 8]
     names = ("h", "totsed", "sed")
@@ -241,12 +241,21 @@ def ensemble_leg(args, ranks):
             scs = [pool.submit(quantized_case(cases[k]), max_steps=cap) for k in subset]
             pool.run(-1)
             env = [s.fields(names) for s in scs]
+    # every compared field must carry something: an empty (all-zero) FP64
+    # field would make any error look perfect
+    from swehr_b200.accuracy import EmptyField
     err = {n: 0.0 for n in names}
     envm = {n: 0.0 for n in names}
+    empty = []
+    wet = []
     for a, b, q in zip(keep["mixed"], keep["fp64"], env):
+        wet.append(float((b["h"] > 1e-4).mean()))
         for n in names:
-            err[n] = max(err[n], rel_linf(a[n], b[n]))
-            envm[n] = max(envm[n], rel_linf(q[n], b[n]))
+            try:
+                err[n] = max(err[n], rel_linf(a[n], b[n], require_nonzero=True))
+                envm[n] = max(envm[n], rel_linf(q[n], b[n], require_nonzero=True))
+            except EmptyField:
+                empty.append(n)
     err = {n: ranks.max(v) for n, v in err.items()}
     envm = {n: ranks.max(v) for n, v in envm.items()}
     # the same scenarios one at a time through the single-domain path
@@ -278,21 +287,24 @@ def ensemble_leg(args, ranks):
                            "sample": f"every {step}th scenario alone, {args.ens_solo_steps} steps each"},
             "mixed_over_batched_fp64": out["mixed"]["value"] / out["fp64"]["value"],
             "mixed_over_solo_fp64": (out["mixed"]["value"] / ranks.world / solo) if solo else None,
-            "error_vs_fp64": {"scenarios": [int(k) for k in range(0, len(all_cases), every)][:8], "rel_linf": err,
-                              "fp32_input_envelope": envm}}
+            "error_vs_fp64": {"scenarios": [int(k) for k in range(0, len(all_cases), every)][:8],
+                              "at_step": cap, "rel_linf": err, "fp32_input_envelope": envm,
+                              "wet_fraction": wet, "empty_fields": sorted(set(empty)),
+                              "valid": not empty and bool(subset)}}
 
 
 def serving_leg(args):
-    """A Poisson request stream through the continuous-batching server.  The
-    default stream is scaled to what one B200 serves in real time; with
-    --serve-full it is the full stream (sides to 2048, up to 10 hyetograph
-    steps, 50/s for 60 s), which offers far more work than one GPU does and
-    is reported by its served fraction."""
+    """A Poisson request stream through the continuous-batching server: the
+    full stream by default (50/s for 60 s, sides to 2048, up to 10
+    hyetograph steps, 150 GB admission limit), which offers more work than
+    one GPU serves and is reported by its served fraction, served for 60 s
+    more after the last arrival; --serve-small scales it to what one B200
+    keeps up with."""
     from swehr_b200 import serving as SV
     from swehr_b200.params import MIXED
-    if args.serve_full:
-        args.serve_side_max, args.serve_hyeto_max = 2048, 10
-        args.serve_duration, args.serve_drain = 60.0, 60.0
+    if args.serve_small:
+        args.serve_side_max, args.serve_hyeto_max = 512, 3
+        args.serve_duration, args.serve_drain = 10.0, 50.0
     reqs = SV.poisson_stream(rate=args.serve_rate, duration=args.serve_duration, seed=3, side_min=32,
                              side_max=args.serve_side_max, hyeto_steps=(1, args.serve_hyeto_max))
     SV.prepare(reqs, SV.TopoBank(3, 2048, 4) if args.serve_side_max > 512 else None)
@@ -321,16 +333,19 @@ def main():
     ap.add_argument("--no-ensemble", action="store_true")
     ap.add_argument("--no-serving", action="store_true")
     ap.add_argument("--ens-count", type=int, default=256)
-    ap.add_argument("--ens-warmup", type=int, default=8)
+    ap.add_argument("--ens-warmup", type=int, default=800,
+                    help="untimed pool steps before the timed ones (the scenarios pond and erode by then)")
     ap.add_argument("--ens-steps", type=int, default=200)
     ap.add_argument("--ens-solo-steps", type=int, default=50)
     ap.add_argument("--serve-rate", type=float, default=50.0)
-    ap.add_argument("--serve-duration", type=float, default=10.0)
-    ap.add_argument("--serve-drain", type=float, default=50.0)
-    ap.add_argument("--serve-side-max", type=int, default=512)
-    ap.add_argument("--serve-hyeto-max", type=int, default=3)
-    ap.add_argument("--serve-full", action="store_true",
-                    help="the full request stream (sides to 2048, 1-10 hyetograph steps, 60 s + 60 s drain)")
+    ap.add_argument("--serve-duration", type=float, default=60.0)
+    ap.add_argument("--serve-drain", type=float, default=60.0)
+    ap.add_argument("--serve-side-max", type=int, default=2048)
+    ap.add_argument("--serve-hyeto-max", type=int, default=10)
+    ap.add_argument("--serve-small", action="store_true",
+                    help="a scaled stream one B200 keeps up with (sides to 512, 1-3 hyetograph steps, 10 s)")
+    ap.add_argument("--steady-at", type=int, default=1000,
+                    help="step at which the second (wet, steady) timed window starts; 0 to skip it")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
@@ -360,7 +375,21 @@ def main():
     S = case.sclass
     cells = case.cells()
 
+    def window(prw, B):
+        """throughput and update-kernel roofline of a timed window"""
+        ms = max_over_ranks(prw.device_ms)
+        n = max(int(prw.steps_this_call), 1)
+        upd = prw.kernel_ms / n
+        ach = B * cells / (upd / 1e3) / 1e9 if upd > 0 else None
+        first = int(prw.steps) - n
+        return {"steps": f"{first}..{int(prw.steps)}", "value": world * cells * n / (ms / 1e3),
+                "unit": "cell-steps/s", "ms_per_step": ms / n, "update_ms_avg": upd, "achieved_gbs": ach,
+                "frac": (ach / hbm_peak()[0]) if ach else None}
+
     def timed_run(precision, clocks=None):
+        """W warm-up steps, K timed steps; then, untimed, on to the steady
+        window (the domain wets up over the first ~1000 steps: dry at step 25,
+        58 % wet at 600, wet everywhere by 1000) and K more timed steps there."""
         sim = Simulation(case, precision=precision)
         sim.advance(max_steps=args.warmup)
         barrier()
@@ -371,11 +400,19 @@ def main():
         sim.set_timing(False)
         clk = clocks.stop() if clocks else None
         barrier()
+        steady = None
+        if args.steady_at > args.warmup + args.steps:
+            sim.advance(max_steps=args.steady_at - (args.warmup + args.steps))
+            barrier()
+            sim.set_timing(True)
+            steady = sim.advance(max_steps=args.steps)
+            sim.set_timing(False)
+            barrier()
         sim.close()
-        return pr, clk
+        return pr, clk, steady
 
     clocks = ClockSampler(local)
-    pr, clk = timed_run(FP64, clocks)
+    pr, clk, st64 = timed_run(FP64, clocks)
     elapsed_ms = max_over_ranks(pr.device_ms)
     kernel_ms = pr.kernel_ms
     steps_done = pr.steps_this_call
@@ -383,7 +420,7 @@ def main():
 
     mixed = None
     if not args.no_mixed:
-        prm, _ = timed_run(MIXED)
+        prm, _, stm = timed_run(MIXED)
         em = max_over_ranks(prm.device_ms)
         vm = world * cells * prm.steps_this_call / (em / 1e3)
         um = prm.kernel_ms / max(prm.steps_this_call, 1)
@@ -399,6 +436,8 @@ def main():
                               "algo_bytes_per_cell_step": Bm, "update_ms_avg": um},
                  "dtype": "f32 bulk; f64 z, infiltration, deposited mass, budgets",
                  "error_bar": "<=1e-4 relative L-inf on depth and concentration vs FP64 (tests/test_gpu_mixed.py)"}
+        if stm is not None:
+            mixed["steady"] = window(stm, algo_bytes_mixed(S))
 
     # end-to-end through the C ABI from host buffers: create (H2D of every
     # input) + the same steps + D2H of every output field, wall-clock
@@ -418,6 +457,10 @@ def main():
         e2e = {"value": e2e_val, "unit": "cell-steps/s", "h2d_bytes_per_step": h2d / n_e2e,
                "d2h_bytes_per_step": d2h / n_e2e,
                "scope": "swehr_create + swehr_advance + swehr_read_field of every output, host buffers"}
+
+    steady = window(st64, algo_bytes_f64(S)) if st64 is not None else None
+    if steady is not None and mixed is not None and mixed.get("steady"):
+        mixed["steady"]["over_fp64"] = mixed["steady"]["value"] / steady["value"]
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -468,6 +511,7 @@ def main():
                          "algo_bytes_per_cell_step": B, "update_ms_avg": upd_ms},
             "cpu_baseline": cpu,
             "e2e": e2e,
+            "steady_state": steady,
             "mixed_form": mixed,
             "batched_ensemble": ensemble,
             "serving": serving,

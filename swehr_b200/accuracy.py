@@ -20,18 +20,29 @@ KEEP64 = {"dx", "tend", "rint", "stageint", "thetas", "theta0", "hf", "ks", "vin
           "storm_peak", "storm_radius", "storm_x0", "storm_y0", "storm_vx", "storm_vy"}
 
 
-def rel_linf(a, b) -> float:
+class EmptyField(ValueError):
+    """The reference field of an error measure is identically zero (or all
+    NaN): a relative error of it says nothing."""
+
+
+def rel_linf(a, b, require_nonzero: bool = False) -> float:
     """max |a - b| / max |b| over positions finite in both (inf if the NaN
-    positions differ)."""
+    positions differ).  When b is zero everywhere the absolute difference is
+    returned -- unless require_nonzero, which raises EmptyField instead, so
+    a comparison of two empty fields cannot pass for an accuracy result."""
     a, b = np.asarray(a), np.asarray(b)
     na, nb = np.isnan(a), np.isnan(b)
     if not np.array_equal(na, nb):
         return float("inf")
     m = ~na
     if not m.any():
+        if require_nonzero:
+            raise EmptyField("no finite values to compare")
         return 0.0
     scale = float(np.max(np.abs(b[m])))
     diff = float(np.max(np.abs(a[m] - b[m])))
+    if scale == 0 and require_nonzero:
+        raise EmptyField("reference field is zero everywhere")
     return diff / scale if scale > 0 else diff
 
 

@@ -168,8 +168,29 @@ class Report:
     def cell_steps_per_s(self) -> float:
         return self.cell_steps / self.wall_s if self.wall_s > 0 else 0.0
 
+    def split(self) -> dict:
+        """Per-request time-to-result split into queueing (arrival ->
+        admission: waiting for HBM or a slot) and residency (admission ->
+        result on the host: the request's steps, shared with everything
+        resident), p50 / p99 / max over the completed requests."""
+        q = [x.admitted - x.arrival for x in self.results]
+        d = [x.finished - x.admitted for x in self.results]
+        out = {}
+        for name, xs in (("queue_s", q), ("resident_s", d)):
+            out[name] = {"p50": percentile(xs, 50), "p99": percentile(xs, 99), "max": max(xs) if xs else None}
+        # the slowest 1 %: how much of their time was queueing
+        lat = sorted(self.results, key=lambda x: x.latency)
+        tail = lat[int(0.99 * len(lat)):] if lat else []
+        out["p99_tail"] = {"n": len(tail),
+                           "queue_share": (sum(x.admitted - x.arrival for x in tail) / sum(x.latency for x in tail))
+                           if tail and sum(x.latency for x in tail) > 0 else None,
+                           "mean_cells": (sum(x.cells for x in tail) / len(tail)) if tail else None,
+                           "mean_steps": (sum(x.steps for x in tail) / len(tail)) if tail else None}
+        return out
+
     def summary(self) -> dict:
         return {"submitted": self.submitted, "completed": self.completed, "incomplete": self.incomplete,
+                "latency_split": self.split(),
                 "rejected": len(self.rejected),
                 "wall_s": self.wall_s, "device_ms": self.device_ms, "cell_steps": self.cell_steps,
                 "pool_steps": self.pool_steps, "cell_steps_per_s": self.cell_steps_per_s,

@@ -2,7 +2,9 @@
 import numpy as np
 
 from swehr_b200 import workloads as W
-from swehr_b200.accuracy import KEEP64, quantized_case, rel_linf
+import pytest
+
+from swehr_b200.accuracy import KEEP64, EmptyField, quantized_case, rel_linf
 
 
 def test_rel_linf():
@@ -14,6 +16,12 @@ def test_rel_linf():
     a[1, 1] = np.nan
     assert rel_linf(a, b) == float("inf")
     assert rel_linf(np.zeros(3), np.zeros(3)) == 0.0
+    # an empty reference field cannot pass for an accuracy result
+    with pytest.raises(EmptyField):
+        rel_linf(np.zeros(3), np.zeros(3), require_nonzero=True)
+    with pytest.raises(EmptyField):
+        rel_linf(np.full(2, np.nan), np.full(2, np.nan), require_nonzero=True)
+    assert rel_linf(np.array([1.0, 2.0]), np.array([1.0, 4.0]), require_nonzero=True) == 0.5
 
 
 def test_quantized_case_rounds_only_fp32_inputs():
