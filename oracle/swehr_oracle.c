@@ -106,6 +106,10 @@ typedef struct orc_ctx {
      * forcing (DFMASK > 0, SWEHR.c:1315-1316) and the debris-flow override of
      * every source (SWEHR.c:1392-1400) */
     int64_t n_fail, n_dfmask, n_debris;
+    /* slab runs (test of the multi-GPU decomposition): rows own_lo..own_hi
+     * are this instance's; its largest wave speed counts only their faces */
+    int own_lo, own_hi;
+    double smax_own, R_step;
 } orc_ctx;
 
 #define IDX(c, i, j) (((size_t)(i) - 1) * (size_t)(c)->ny + ((size_t)(j) - 1))
@@ -273,7 +277,9 @@ static double orc_spe(double uh, double vh, double h, double beta, double rho, d
     return E;
 }
 
-static int orc_step(orc_ctx *c)
+/* Phases 1-3 of a step (slopes, faces, sources); the largest wave speed of
+ * the owned faces goes to c->smax_own.  orc_commit finishes the step. */
+static void orc_prepare(orc_ctx *c)
 {
     const swehr_params *p = &c->p;
     const int nx = c->nx, ny = c->ny, S = c->S, N = c->N, NF = 3 + S;
@@ -334,7 +340,7 @@ static int orc_step(orc_ctx *c)
                 f[0] = T[0]; f[1] = T[1]; f[2] = T[2];
                 for (int k = 0; k < S; k++)
                     f[3 + k] = (T[0] > 0) ? T[0] * orc_nbsed(&L, k) : T[0] * orc_nbsed(&Rn, k);
-                if (s > smax) smax = s;
+                if (s > smax && ((i >= c->own_lo && i <= c->own_hi) || (i == 0 && c->own_lo == 1))) smax = s;
             }
             if (i != 0) { /* y face j+1/2 */
                 orc_neighbour(c, i, j, inflow, sedin, &L);
@@ -350,7 +356,7 @@ static int orc_step(orc_ctx *c)
                 f[0] = T[0]; f[1] = T[2]; f[2] = T[1];
                 for (int k = 0; k < S; k++)
                     f[3 + k] = (T[0] > 0) ? T[0] * orc_nbsed(&L, k) : T[0] * orc_nbsed(&Rn, k);
-                if (s > smax) smax = s;
+                if (s > smax && i >= c->own_lo && i <= c->own_hi) smax = s;
             }
         }
     }
@@ -457,6 +463,21 @@ static int orc_step(orc_ctx *c)
     c->n_fail += n_fail;
     c->n_dfmask += n_dfmask;
     c->n_debris += n_debris;
+    c->smax_own = smax;
+    c->R_step = R;
+}
+
+/* The rest of a step given the largest wave speed over every face of the
+ * domain: the CFL time step, the cell update, time and series. */
+static int orc_commit(orc_ctx *c, double smax)
+{
+    const swehr_params *p = &c->p;
+    const int nx = c->nx, ny = c->ny, S = c->S, N = c->N, NF = 3 + S;
+    const double oneoverdx = 1 / p->dx;
+    const double hfilm = p->hfilm, rhos = p->rhos, rhow = p->rhow, phi = p->phi;
+    const double t = c->t;
+    const int storm = p->storm_peak > 0;
+    const double R = c->R_step;
 
     /* CFL time step (SWEHR.c:1409-1413) */
     double dt = p->cstable * p->dx / smax;
@@ -666,6 +687,12 @@ static int orc_step(orc_ctx *c)
     return cfl ? SWEHR_CFL_ERROR : SWEHR_OK;
 }
 
+static int orc_step(orc_ctx *c)
+{
+    orc_prepare(c);
+    return orc_commit(c, c->smax_own);
+}
+
 /* ---------------------------------------------------------------- ABI --- */
 
 static void *orc_alloc(size_t n)
@@ -723,6 +750,8 @@ orc_ctx *orc_create(const swehr_params *p, const swehr_inputs *in)
         c->vinf[q] = p->vinf0;
         c->rho[q] = p->rhow * (1 - 0.0) + p->rhos * 0.0;   /* initialcondition, SWEHR.c:270 */
     }
+    c->own_lo = 1;
+    c->own_hi = c->nx;
     c->stagecap = 200000;
     c->stage = (double *)orc_alloc((size_t)c->stagecap * ORC_STAGE_COLS);
     c->saveflow = (double *)orc_alloc((size_t)c->stagecap * ORC_POINT_COLS);
@@ -832,6 +861,52 @@ int orc_get_budget(orc_ctx *c, swehr_budget *b)
 }
 
 double orc_time(orc_ctx *c) { return c->t; }
+
+/* Slab runs: own rows lo..hi (1-based) -- only their faces enter the wave
+ * speed; orc_step_prepare returns that speed, orc_step_commit finishes the
+ * step with the largest one over all slabs; orc_rows copies every state
+ * array of rows lo..hi out of (set = 0) or into (set = 1) buf, in the order
+ * h hu hv z zp vinf maxvel maxdep totm dep totsed rho, then U_k, M_k, SED_k
+ * per class: (12 + 3S) * ny values per row. */
+void orc_set_own(orc_ctx *c, int lo, int hi)
+{
+    c->own_lo = lo;
+    c->own_hi = hi;
+}
+
+double orc_step_prepare(orc_ctx *c)
+{
+    orc_prepare(c);
+    return c->smax_own;
+}
+
+int orc_step_commit(orc_ctx *c, double smax)
+{
+    int st = orc_commit(c, smax);
+    if (st != SWEHR_OK) c->status = st;
+    return st;
+}
+
+int orc_rows(orc_ctx *c, int lo, int hi, double *buf, int set)
+{
+    if (lo < 1 || hi > c->nx || lo > hi) return SWEHR_INVALID;
+    const size_t ny = (size_t)c->ny, N = (size_t)c->N, n = (size_t)(hi - lo + 1) * ny, off = (size_t)(lo - 1) * ny;
+    double *planes[12] = {c->h, c->hu, c->hv, c->z, c->zp, c->vinf, c->maxvel, c->maxdep,
+                          c->totm, c->dep, c->totsed, c->rho};
+    size_t pos = 0;
+    for (int f = 0; f < 12; f++, pos += n) {
+        if (set) memcpy(planes[f] + off, buf + pos, n * sizeof(double));
+        else memcpy(buf + pos, planes[f] + off, n * sizeof(double));
+    }
+    double *groups[3] = {c->U, c->M, c->sed};
+    for (int g = 0; g < 3; g++)
+        for (int k = 0; k < c->S; k++, pos += n) {
+            double *pl = groups[g] + (size_t)k * N + off;
+            if (set) memcpy(pl, buf + pos, n * sizeof(double));
+            else memcpy(buf + pos, pl, n * sizeof(double));
+        }
+    return SWEHR_OK;
+}
 
 /* branch counters: 0 slope failures, 1 cells with debris forcing (DFMASK > 0),
  * 2 cells under the debris-flow override; cell-steps since creation */
