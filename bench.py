@@ -233,6 +233,7 @@ def ensemble_leg(args, ranks):
             out[label] = {"value": cs / (dev_ms / 1e3), "unit": "cell-steps/s", "pool_steps": int(st.pool_steps),
                           "device_ms": dev_ms, "ms_per_pool_step": dev_ms / max(st.pool_steps, 1),
                           "grid_wave": int(tu.grid_wave), "grid_update": int(tu.grid_update),
+                          "tile": f"{int(tu.tile_i)}x{int(tu.tile_j)}",
                           "upload_s": upload_s, "hbm_bytes_rank0": int(st.hbm_used)}
     # envelope: FP64 on the subset's inputs rounded to FP32
     env = []

@@ -247,6 +247,7 @@ typedef struct {
     double device_ms;        /* GPU time of this call */
     size_t hbm_used, hbm_limit;
     int32_t grid_wave, grid_update;   /* launch shape in use (blocks) */
+    int32_t tile_i, tile_j;           /* tile shape in use (cells; 8 x 32 or 16 x 16) */
 } swehr_pool_stats;
 
 /* precision: SWEHR_FP64 or SWEHR_MIXED for every scenario; max_classes:
@@ -268,8 +269,11 @@ int swehr_pool_submit(swehr_pool *pool, const swehr_params *p, const swehr_input
 int swehr_pool_run(swehr_pool *pool, int64_t steps, swehr_pool_stats *stats);
 
 /* Launch-shape autotuner: times `steps_per_trial` real pool steps for each
- * candidate persistent grid (1..occupancy blocks per SM for each kernel) and
- * keeps the fastest per tile-step; the scenarios advance meanwhile. */
+ * candidate -- tile shape (8 x 32 or 16 x 16 cells) and persistent grid
+ * (1..occupancy blocks per SM for each kernel) -- in three round-robin
+ * passes, and keeps the shape and grids with the least time per running
+ * cell; the scenarios advance meanwhile, with results that do not depend on
+ * the candidate (bit for bit in the FP64 form). */
 int swehr_pool_tune(swehr_pool *pool, int64_t steps_per_trial, swehr_pool_stats *stats);
 
 /* progress of one scenario (status, done, t, steps) */

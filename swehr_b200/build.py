@@ -29,6 +29,8 @@ SOURCES = [
     ("swehr_capi.cu", []),
     ("swehr_pool.cu", []),
     ("swehr_cfl_noalloc.cu", ["--fmad=false"]),
+    ("swehr_batch16_f64.cu", ["--fmad=false"]),
+    ("swehr_batch16_f32.cu", []),
 ]
 
 

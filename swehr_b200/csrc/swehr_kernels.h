@@ -72,6 +72,9 @@ struct BatchConfig {
 
 int configure_batch_f64(int max_classes, bool budget, BatchConfig &cfg);
 int configure_batch_f32(int max_classes, bool budget, BatchConfig &cfg);
+/* the same kernels built for 16 x 16-cell tiles (cfg.tile_i = cfg.tile_j = 16) */
+int configure_batch_f64_t16(int max_classes, bool budget, BatchConfig &cfg);
+int configure_batch_f32_t16(int max_classes, bool budget, BatchConfig &cfg);
 
 /* launch geometry of the step kernels of one simulation */
 struct StepConfig {

@@ -10,6 +10,7 @@
 #include "swehr_tile.cuh"
 
 namespace swehr {
+inline namespace SWEHR_TILE_NS {
 
 template <class PP, class RS>
 struct FormLauncher {
@@ -153,4 +154,5 @@ struct FormLauncher {
     }
 };
 
+}  // inline namespace SWEHR_TILE_NS
 }  // namespace swehr

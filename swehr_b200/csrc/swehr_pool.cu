@@ -52,7 +52,9 @@ int64_t tiles_of(const DevParams &P, const BatchConfig &c)
 struct swehr_pool {
     int device = 0, num_sms = 148, precision = SWEHR_FP64, max_classes = 1, budget = 0, max_scen = 0;
     size_t hbm_limit = 0, hbm_used = 0;
-    BatchConfig cfg;
+    BatchConfig cfg;                     /* the tile shape in use (a copy of shapes[shape]) */
+    BatchConfig shapes[2];               /* 8 x 32 and 16 x 16 tiles */
+    int shape = 0;
     int grid_wave = 0, grid_update = 0, tuned = 0;
     int kw_sel = 0, ku_sel = 0;          /* tuned blocks per SM (0: occupancy) */
     int max_s = 1;                       /* largest class count running */
@@ -208,6 +210,7 @@ static int rebuild_table(swehr_pool *pl)
     for (auto &s : pl->scen) {
         if (!s.running) continue;
         max_s = std::max(max_s, (int)s.ctx->P.S);
+        s.ntiles = tiles_of(s.ctx->P, pl->cfg);     /* in the tile shape in use */
         char *slot = pl->h_tab + (size_t)k * pl->desc_bytes;
         if (pl->precision == SWEHR_MIXED)
             fill_desc<float>(s, s.ctx->B32, pl->d_sum, tile0, (ScenDesc<float> *)slot);
@@ -347,6 +350,8 @@ static void fill_stats(swehr_pool *pl, swehr_pool_stats *st)
     st->hbm_limit = pl->hbm_limit;
     st->grid_wave = pl->grid_wave;
     st->grid_update = pl->grid_update;
+    st->tile_i = pl->cfg.tile_i;
+    st->tile_j = pl->cfg.tile_j;
 }
 
 static PoolScen *find(swehr_pool *pl, int id)
@@ -389,8 +394,13 @@ int swehr_pool_create(int precision, int max_classes, int budget, size_t hbm_lim
     PCKF(cudaGetDevice(&pl->device));
     PCKF(cudaDeviceGetAttribute(&pl->num_sms, cudaDevAttrMultiProcessorCount, pl->device));
     {
-        int ce = precision == SWEHR_MIXED ? configure_batch_f32(max_classes, pl->budget != 0, pl->cfg)
-                                          : configure_batch_f64(max_classes, pl->budget != 0, pl->cfg);
+        const bool b = pl->budget != 0;
+        int ce = precision == SWEHR_MIXED ? configure_batch_f32(max_classes, b, pl->shapes[0])
+                                          : configure_batch_f64(max_classes, b, pl->shapes[0]);
+        if (!ce)
+            ce = precision == SWEHR_MIXED ? configure_batch_f32_t16(max_classes, b, pl->shapes[1])
+                                          : configure_batch_f64_t16(max_classes, b, pl->shapes[1]);
+        pl->cfg = pl->shapes[0];
         if (ce) {
             rc = swehr_err(SWEHR_CUDA_ERROR, std::string("configure: ") + cudaGetErrorString((cudaError_t)ce));
             pool_free(pl);
@@ -542,29 +552,50 @@ int swehr_pool_tune(swehr_pool *pl, int64_t steps_per_trial, swehr_pool_stats *s
         int rc = rebuild_table(pl);
         if (rc) return rc;
     }
-    const int occ_u = pl->cfg.occ_update_s[pl->max_s];
-    const int trials = std::max(pl->cfg.occ_wave, occ_u);
     const size_t need = (size_t)3 * steps_per_trial;
     while (pl->ev_ring.size() < need) {
         cudaEvent_t e;
         PCK(cudaEventCreate(&e));
         pl->ev_ring.push_back(e);
     }
-    /* every candidate is timed in each of kRounds round-robin passes and
-     * keeps its best time per tile, so the state drifting between trials
-     * and one-off noise do not decide */
+    /* Candidates: each tile shape with 1..occupancy blocks per SM for each
+     * kernel.  Every candidate runs steps_per_trial real pool steps in each
+     * of kRounds round-robin passes and keeps its best time per running cell
+     * (cells, not tiles: the shapes cut the same scenarios into different
+     * tile counts), so the state drifting between trials and one-off noise
+     * do not decide.  A shape's best wave and update grids are chosen
+     * separately; the shape with the smaller sum wins. */
     const int kRounds = 3;
-    std::vector<double> bw((size_t)trials + 1, INFINITY), bu((size_t)trials + 1, INFINITY);
-    for (int trial = 0; trial < kRounds * trials; trial++) {
-        const int k = 1 + trial % trials;
+    const int nsh = 2;
+    int trials[2], occ_u[2];
+    std::vector<std::pair<int, int>> cand;
+    for (int sh = 0; sh < nsh; sh++) {
+        occ_u[sh] = pl->shapes[sh].occ_update_s[pl->max_s];
+        trials[sh] = std::max(pl->shapes[sh].occ_wave, occ_u[sh]);
+        for (int k = 1; k <= trials[sh]; k++) cand.push_back({sh, k});
+    }
+    std::vector<double> bw[2], bu[2];
+    for (int sh = 0; sh < nsh; sh++) {
+        bw[sh].assign((size_t)trials[sh] + 1, INFINITY);
+        bu[sh].assign((size_t)trials[sh] + 1, INFINITY);
+    }
+    auto use_shape = [&](int sh) {
+        if (pl->shape == sh) return;
+        pl->shape = sh;
+        pl->cfg = pl->shapes[sh];
+        pl->dirty = true;                /* tile counts change: rebuild the table */
+    };
+    for (int trial = 0; trial < kRounds * (int)cand.size(); trial++) {
+        const int sh = cand[trial % cand.size()].first, k = cand[trial % cand.size()].second;
+        use_shape(sh);
         if (pl->dirty) {
             int rc = rebuild_table(pl);
             if (rc) return rc;
         }
         if (pl->nrun == 0) break;
-        const int kw = std::min(k, pl->cfg.occ_wave), ku = std::min(k, occ_u);
+        const int kw = std::min(k, pl->cfg.occ_wave), ku = std::min(k, occ_u[sh]);
         set_grids(pl, kw, ku);
-        const int64_t tiles = pl->total_tiles;
+        const double cells = (double)std::max<int64_t>(pl->running_cells, 1);
         for (int64_t s = 0; s < steps_per_trial; s++)
             launch_pool_step(pl, pl->ev_ring[3 * s], pl->ev_ring[3 * s + 1], pl->ev_ring[3 * s + 2]);
         PCK(cudaGetLastError());
@@ -580,19 +611,32 @@ int swehr_pool_tune(swehr_pool *pl, int64_t steps_per_trial, swehr_pool_stats *s
             u += b;
         }
         local.device_ms += w + u;
-        w /= (double)tiles;
-        u /= (double)tiles;
-        if (kw == k) bw[k] = std::min(bw[k], w);
-        if (ku == k) bu[k] = std::min(bu[k], u);
+        if (kw == k) bw[sh][k] = std::min(bw[sh][k], w / cells);
+        if (ku == k) bu[sh][k] = std::min(bu[sh][k], u / cells);
     }
-    int kw_best = pl->cfg.occ_wave, ku_best = occ_u;
-    for (int k = 1; k <= trials; k++) {
-        if (bw[k] < bw[kw_best]) kw_best = k;
-        if (bu[k] < bu[ku_best]) ku_best = k;
+    int best_sh = 0, kw_best[2], ku_best[2];
+    double best_t = INFINITY;
+    for (int sh = 0; sh < nsh; sh++) {
+        kw_best[sh] = pl->shapes[sh].occ_wave;
+        ku_best[sh] = occ_u[sh];
+        for (int k = 1; k <= trials[sh]; k++) {
+            if (bw[sh][k] < bw[sh][kw_best[sh]]) kw_best[sh] = k;
+            if (bu[sh][k] < bu[sh][ku_best[sh]]) ku_best[sh] = k;
+        }
+        const double t = bw[sh][kw_best[sh]] + bu[sh][ku_best[sh]];
+        if (t < best_t) {
+            best_t = t;
+            best_sh = sh;
+        }
     }
-    pl->kw_sel = kw_best;
-    pl->ku_sel = ku_best;
-    set_grids(pl, kw_best, ku_best);
+    use_shape(best_sh);
+    pl->kw_sel = kw_best[best_sh];
+    pl->ku_sel = ku_best[best_sh];
+    if (pl->dirty) {
+        int rc = rebuild_table(pl);
+        if (rc) return rc;
+    }
+    set_grids(pl, pl->kw_sel, std::min(pl->ku_sel, occ_u[best_sh]));
     pl->tuned = 1;
     fill_stats(pl, &local);
     if (st) *st = local;

@@ -35,10 +35,25 @@
 
 #include <cuda_pipeline_primitives.h>
 
-namespace swehr {
+/* Tile shape: T_I x T_J cells, one per thread of a 256-thread block.  A
+ * translation unit may build the kernels for another shape by defining
+ * SWEHR_TILE_I, SWEHR_TILE_J and SWEHR_TILE_NS before including this
+ * header: everything below then lives in the inline namespace
+ * swehr::SWEHR_TILE_NS, so two shapes in one library never share a symbol.
+ * The per-cell arithmetic does not depend on the shape. */
+#ifndef SWEHR_TILE_I
+#define SWEHR_TILE_I 8
+#define SWEHR_TILE_J 32
+#define SWEHR_TILE_NS t8x32
+#endif
+static_assert(SWEHR_TILE_I * SWEHR_TILE_J == 256, "a tile is one cell per thread of a 256-thread block");
+static_assert(SWEHR_TILE_J % 4 == 0, "staged rows start 16-byte aligned");
 
-#define T_I 8
-#define T_J 32
+namespace swehr {
+inline namespace SWEHR_TILE_NS {
+
+#define T_I SWEHR_TILE_I
+#define T_J SWEHR_TILE_J
 #define H_I (T_I + 2)
 #define H_J (T_J + 2)
 #define N_H (H_I * H_J)
@@ -222,13 +237,13 @@ __device__ __forceinline__ TileCoord tile_coord(const DevParams &P, int64_t tile
  *   topography   z_prev 12 x 36, z 10 x 36
  * Row r of a halo plane is grid row i0-1+r; column c is grid column
  * (0-based) j0-3+c, so halo cell (hi, hj) sits at (hi, hj+1) and the first
- * column is 16-byte aligned.  Rows or columns outside the grid are not
+ * column is 16-byte aligned.  (Counts above are for the 8 x 32 tile.)  Rows or columns outside the grid are not
  * loaded: ghosts are resolved from their source cells afterwards
  * (SWEHR.c:816-1035). */
-#define R_J 36              /* staged columns */
-#define HALO_ROWS H_I       /* 10 */
-#define ZP_ROWS 12
-#define ZC_ROWS 10
+#define R_J (T_J + 4)       /* staged columns */
+#define HALO_ROWS H_I
+#define ZP_ROWS (T_I + 4)
+#define ZC_ROWS (T_I + 2)
 
 static_assert((size_t)(TILE_THREADS / 32) * B_NTERMS * sizeof(double) <= 4 * N_H * sizeof(float),
               "budget reduction fits in the face-state arrays it reuses");
@@ -312,7 +327,9 @@ __device__ __forceinline__ void stage_load(const DevParams &P, const SetV<RS> &s
     if (tid < HALO_ROWS * (R_J / 2)) {
         const int r = tid / (R_J / 2), k2 = tid - r * (R_J / 2);
         const int gi = tc.i0 - 1 + r, col = c0 + 2 * k2;
-        if (gi >= 1 && gi <= P.nx && col >= 0 && col < P.pitch) {
+        /* columns past ny are row padding no cell reads (a ghost column
+         * takes its source cell's values): not loaded */
+        if (gi >= 1 && gi <= P.nx && col >= 0 && col < P.ny) {
             const int64_t go = (int64_t)(gi - 1) * P.pitch + col;
             RS *d = reinterpret_cast<RS *>(smb + L.halo) + r * R_J + 2 * k2;
             const int ps = HALO_ROWS * R_J;
@@ -334,7 +351,7 @@ __device__ __forceinline__ void stage_load(const DevParams &P, const SetV<RS> &s
             const int s2 = isp ? s : s - ZP_ROWS * (R_J / 2);
             const int r = s2 / (R_J / 2), k2 = s2 - r * (R_J / 2);
             const int gi = (isp ? tc.i0 - 2 : tc.i0 - 1) + r, col = c0 + 2 * k2;
-            if (gi < 1 || gi > P.nx || col < 0 || col >= P.pitch) continue;
+            if (gi < 1 || gi > P.nx || col < 0 || col >= P.ny) continue;
             double *d = reinterpret_cast<double *>(smb + (isp ? L.zp : L.zc)) + r * R_J + 2 * k2;
             cp_pair(d, (isp ? zp : zc) + (int64_t)(gi - 1) * P.pitch + col);
         }
@@ -344,7 +361,7 @@ __device__ __forceinline__ void stage_load(const DevParams &P, const SetV<RS> &s
         const int s = tid - (TILE_THREADS - T_I * (T_J / 2));
         const int r = s / (T_J / 2), k2 = s - r * (T_J / 2);
         const int gi = tc.i0 + r, col = tc.j0 - 1 + 2 * k2;
-        if (gi <= P.nx && col < P.pitch) {
+        if (gi <= P.nx && col < P.ny) {
             const int64_t go = (int64_t)(gi - 1) * P.pitch + col;
             RS *cr = reinterpret_cast<RS *>(smb + L.cell_r) + r * T_J + 2 * k2;
             double *cd = reinterpret_cast<double *>(smb + L.cell_d) + r * T_J + 2 * k2;
@@ -1546,4 +1563,5 @@ __global__ void __launch_bounds__(TILE_THREADS, PP::kMinBlocks) k_update_batch(c
     if (run) flush();
 }
 
+}  // inline namespace SWEHR_TILE_NS
 }  // namespace swehr

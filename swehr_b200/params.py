@@ -85,6 +85,7 @@ class SwehrPoolStats(C.Structure):
         ("pool_steps", C.c_int64), ("cell_steps", C.c_int64), ("device_ms", C.c_double),
         ("hbm_used", C.c_size_t), ("hbm_limit", C.c_size_t),
         ("grid_wave", C.c_int32), ("grid_update", C.c_int32),
+        ("tile_i", C.c_int32), ("tile_j", C.c_int32),
     ]
 
 

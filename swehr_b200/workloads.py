@@ -149,10 +149,12 @@ def fractal_domain(nx: int = 4096, ny: int = 4096, dx: float = 2.0, seed: int = 
     return Case(f"fractal{nx}x{ny}", params, topo, rain, ds, pf, ks=ks, max_steps=steps)
 
 
-def ensemble(count: int = 256, seed: int = 2, side_min: int = 64, side_max: int = 1024):
+def ensemble(count: int = 256, seed: int = 2, side_min: int = 64, side_max: int = 1024, only=None):
     """Independent square catchments for batched runs: sides log-uniform,
     dx = 1 m, per-scenario fractal seeds, rain U(20,150) mm/h for U(300,1800) s,
-    Manning n U(0.02, 0.08), 7 classes; each runs to the end of its event."""
+    Manning n U(0.02, 0.08), 7 classes; each runs to the end of its event.
+    only: indices whose topography is generated (the others are None in the
+    returned list; their parameters are drawn all the same)."""
     rng = np.random.default_rng(seed)
     sides = np.exp(rng.uniform(math.log(side_min), math.log(side_max), size=count)).astype(int)
     cases = []
@@ -162,6 +164,9 @@ def ensemble(count: int = 256, seed: int = 2, side_min: int = 64, side_max: int 
         intensity = rng.uniform(20.0, 150.0) * MMH
         duration = float(rng.uniform(300.0, 1800.0))
         n = float(rng.uniform(0.02, 0.08))
+        if only is not None and s not in only:
+            cases.append(None)
+            continue
         topo = fractal_topo(side, side, 1.0, 0.8, 40.0, 0.03, 1000 + s)
         params = common_soil(nx=side, ny=side, dx=1.0, tend=duration, rnum=1, rint=duration,
                              sclass=7, roughness=n, manning0=n)

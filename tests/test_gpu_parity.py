@@ -8,6 +8,8 @@ libm's last-bit rounding; those tests assert the north-star bar of 1e-10
 relative L-infinity where the reference's own floor allows it, and report
 the measured value.
 """
+import os
+
 import numpy as np
 import pytest
 
@@ -225,22 +227,36 @@ def test_solid_cells_mixed_and_pool():
 
 
 def _mem_available_gb() -> float:
+    """Host memory this process may still use: MemAvailable, capped by the
+    container's cgroup limit (a container sees the whole host's meminfo)."""
+    avail = 0.0
     try:
         for line in open("/proc/meminfo"):
             if line.startswith("MemAvailable:"):
-                return int(line.split()[1]) / 2 ** 20
+                avail = int(line.split()[1]) / 2 ** 20
     except OSError:
         pass
-    return 0.0
+    for path, used in (("/sys/fs/cgroup/memory.max", "/sys/fs/cgroup/memory.current"),
+                       ("/sys/fs/cgroup/memory/memory.limit_in_bytes", "/sys/fs/cgroup/memory/memory.usage_in_bytes")):
+        try:
+            lim = open(path).read().strip()
+            if lim != "max":
+                cur = int(open(used).read().strip()) if os.path.exists(used) else 0
+                avail = min(avail, (int(lim) - cur) / 2 ** 30)
+        except (OSError, ValueError):
+            pass
+    return avail
 
 
 def test_roofline_domain_bitexact():
     """The 4096x4096 roofline domain (state planes of 134 MB, offsets past
     2^31 bytes) for 20 steps against the oracle (all host threads), field by
     field.  The oracle holds ~14 GB of host memory at this size; with less
-    than 40 GB available the 2048x2048 corner of the same domain runs
-    instead (said in the output)."""
-    n = 4096 if _mem_available_gb() >= 40 else 2048
+    than 48 GB available to this process (cgroup limit included) the
+    2048x2048 corner of the same domain runs instead, and with less than
+    12 GB the 1024x1024 corner (said in the output)."""
+    gb = _mem_available_gb()
+    n = 4096 if gb >= 48 else (2048 if gb >= 12 else 1024)
     c = W.fractal_domain(nx=4096, ny=4096, dx=2.0, steps=20)
     if n != 4096:
         c = W.Case(c.name + "_corner", dict(c.params, nx=n, ny=n), c.topo[:n, :n].copy(), c.rain, c.ds, c.pfrac,
@@ -271,7 +287,7 @@ def test_pool_ensemble_scenarios_to_event_end():
     bit.  These fractal catchments pond, erode, deposit and fail on their
     steep slopes well before their events end."""
     from swehr_b200.lib import Pool
-    cases = W.ensemble(256)
+    cases = W.ensemble(256, only=ENSEMBLE_TO_END)
     picked = [cases[k] for k in ENSEMBLE_TO_END]
     with Pool(precision=0, max_classes=8, max_scenarios=8) as pool:
         scs = [pool.submit(c) for c in picked]

@@ -65,6 +65,8 @@ def _pool_all(cases, precision, join_after=None, tune=False, max_classes=8):
             if tune and step == 0:
                 st = pool.tune(4)
                 assert st.tuned == 1 and st.grid_update > 0 and st.grid_wave > 0
+                # the tuner ran real steps in both tile shapes and kept one
+                assert (st.tile_i, st.tile_j) in ((8, 32), (16, 16))
                 step += st.pool_steps
             else:
                 nxt = min([join_after[k] for k in pending], default=step + 10 ** 9)
