@@ -953,20 +953,15 @@ __device__ __forceinline__ void tile_cell(const DevParams &P, const SetV<RS> &sr
             uflux = Ureg[kSlot ? 0 : k];
         const double Mk0 = L.stage_m ? celld[(CD_M + k) * T_I * T_J + cs] : __ldg(src.M + qm);
         const R Mk0r = (R)Mk0;
-        R E1 = 0, E2 = 0, E3 = 0, E4 = 0;
-        if (swash) {
+        /* Rain-splash detachment of the original soil is the only source the
+         * shallow branch uses; the other sources and the settling velocity
+         * are formed only in the deep branch, where they are read (the same
+         * values, computed only when needed). */
+        R E1 = 0;
+        if (swash && !debris) {
             E1 = (1 - Hs) * K.pf[k] * K.a * Rc;
-            if (totm0 > R(1e-8) && Mk0r > R(1e-8)) E2 = PP::div(Hs * Mk0r, totm0) * K.ad * Rc;
-            if (deepv) { E1 = E1 * depthfac; E2 = E2 * depthfac; }
-            E3 = PP::div((1 - Hs) * K.pf[k] * K.F, K.J) * (h0v > K.ds[k] ? E3b : R(0));
-            if (totm0 > R(1e-6) && Mk0r > 0)
-                E4 = PP::div(PP::div(K.one_m_bb * Hs * Mk0r, totm0) * K.F, e4den) * (h0v > K.ds[k] ? E4b : R(0));
+            if (deepv) E1 = E1 * depthfac;
         }
-        R VF = PP::settle(K.a13[k], K.a13sq[k], K.c109s * gz * K.ds[k]);
-        VF = VF * vfconc;
-        if (K.ds[k] > R(0.0001) && h0v < K.h0x9) VF = R(2e-3) + PP::div(fmax(h0v - K.h0x3, R(0)) * (VF - R(2e-3)), K.h0x6);
-        if (K.ds[k] > R(0.002) && h0v < K.h0x9) VF = R(2e-3) + PP::div(fmax(h0v - K.h0x3, R(0)) * (VF - R(2e-3)), K.h0x6);
-        if (debris) { E1 = E2 = E3 = E4 = 0; VF = 0; }
 
         double Mk = Mk0;
         R u = uflux;
@@ -976,6 +971,20 @@ __device__ __forceinline__ void tile_cell(const DevParams &P, const SetV<RS> &sr
             u = 0;
             if (BUDGET) det_k = (double)(dtr * E1);
         } else {
+            R E2 = 0, E3 = 0, E4 = 0, VF = 0;
+            if (swash && !debris) {
+                if (totm0 > R(1e-8) && Mk0r > R(1e-8)) E2 = PP::div(Hs * Mk0r, totm0) * K.ad * Rc;
+                if (deepv) E2 = E2 * depthfac;
+                E3 = PP::div((1 - Hs) * K.pf[k] * K.F, K.J) * (h0v > K.ds[k] ? E3b : R(0));
+                if (totm0 > R(1e-6) && Mk0r > 0)
+                    E4 = PP::div(PP::div(K.one_m_bb * Hs * Mk0r, totm0) * K.F, e4den) * (h0v > K.ds[k] ? E4b : R(0));
+            }
+            if (!debris) {
+                VF = PP::settle(K.a13[k], K.a13sq[k], K.c109s * gz * K.ds[k]);
+                VF = VF * vfconc;
+                if (K.ds[k] > R(0.0001) && h0v < K.h0x9) VF = R(2e-3) + PP::div(fmax(h0v - K.h0x3, R(0)) * (VF - R(2e-3)), K.h0x6);
+                if (K.ds[k] > R(0.002) && h0v < K.h0x9) VF = R(2e-3) + PP::div(fmax(h0v - K.h0x3, R(0)) * (VF - R(2e-3)), K.h0x6);
+            }
             chtemp = u;
             const R redetach = fmin(Mk0r, dtr * (E2 + E4));
             const R dec = PP::exp(PP::div(-VF, h) * (half * dtr));

@@ -276,9 +276,12 @@ def test_roofline_domain_bitexact():
                 assert np.array_equal(a, b, equal_nan=True), (name, k)
 
 
-# the smallest scenarios of the 256-scenario ensemble (sides 64-66, events of
-# 427-1168 s at 30-140 mm/h), each run to the end of its event
-ENSEMBLE_TO_END = (141, 86, 84, 215)
+# four of the smallest scenarios of the 256-scenario ensemble (sides 64-67),
+# each run to the end of its event: 141 (427 s at 131 mm/h, 25 k steps, slope
+# failure), 64 (1497 s at 43 mm/h, 42 k steps, failure and debris forcing),
+# 97 (1704 s at 46 mm/h, 134 k steps, failure, debris forcing and the
+# debris-flow override) and 187 (1053 s at 29 mm/h: all infiltrates, 4 k dry steps)
+ENSEMBLE_TO_END = (141, 64, 97, 187)
 
 
 def test_pool_ensemble_scenarios_to_event_end():
@@ -289,6 +292,7 @@ def test_pool_ensemble_scenarios_to_event_end():
     from swehr_b200.lib import Pool
     cases = W.ensemble(256, only=ENSEMBLE_TO_END)
     picked = [cases[k] for k in ENSEMBLE_TO_END]
+    counts = []
     with Pool(precision=0, max_classes=8, max_scenarios=8) as pool:
         scs = [pool.submit(c) for c in picked]
         assert all(s is not None for s in scs)
@@ -299,5 +303,7 @@ def test_pool_ensemble_scenarios_to_event_end():
             o = OracleRun(c, "shim")
             o.advance()
             assert o.steps == pr.steps and o.t == pr.t, (k, o.steps, pr.steps)
-            assert o.counters()["fail"] > 0 or float(o.field("totsed").max()) > 0, k
             _assert_bitexact(sc.fields(), o.fields())
+            counts.append(o.counters())
+    assert sum(c["fail"] > 0 for c in counts) >= 3 and sum(c["dfmask"] > 0 for c in counts) >= 2
+    assert any(c["debris"] > 0 for c in counts)
