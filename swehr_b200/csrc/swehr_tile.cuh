@@ -749,9 +749,11 @@ __device__ __forceinline__ typename PP::R storm_r(const DevParams &P, double t, 
 /* A solid cell in the update (SWEHR.c:1421 false branch, 1566-1574): no
  * water, momentum or suspended sediment; everything else -- deposit,
  * infiltration, topography, maxima, its GZ -- as it was.  What a written
- * state held there leaves the budget as outflow. */
+ * state held there leaves the budget as outflow.  (Inlined: a call taking
+ * the kernel's parameter block by reference would copy all of it to local
+ * memory in every thread.) */
 template <class PP, class RS, int MAXS, bool BUDGET>
-__device__ __noinline__ void solid_cell(const DevParams &P, const SetV<RS> &src, const SetV<RS> &dst,
+__device__ __forceinline__ void solid_cell(const DevParams &P, const SetV<RS> &src, const SetV<RS> &dst,
                                         const double *__restrict__ zc, double *__restrict__ zn, int64_t q,
                                         Acc2<MAXS, BUDGET> &acc)
 {
