@@ -244,21 +244,26 @@ def ensemble_leg(args, ranks):
             env = [s.fields(names) for s in scs]
     # every compared field must carry something: an empty (all-zero) FP64
     # field would make any error look perfect
+    # field: an all-zero FP64 field (a scenario that has not ponded yet
+    # carries no sediment) is skipped and counted, never scored as a match
     from swehr_b200.accuracy import EmptyField
     err = {n: 0.0 for n in names}
     envm = {n: 0.0 for n in names}
-    empty = []
+    compared = {n: 0 for n in names}
     wet = []
     for a, b, q in zip(keep["mixed"], keep["fp64"], env):
         wet.append(float((b["h"] > 1e-4).mean()))
         for n in names:
             try:
-                err[n] = max(err[n], rel_linf(a[n], b[n], require_nonzero=True))
-                envm[n] = max(envm[n], rel_linf(q[n], b[n], require_nonzero=True))
+                e = rel_linf(a[n], b[n], require_nonzero=True)
+                v = rel_linf(q[n], b[n], require_nonzero=True)
             except EmptyField:
-                empty.append(n)
+                continue
+            err[n], envm[n] = max(err[n], e), max(envm[n], v)
+            compared[n] += 1
     err = {n: ranks.max(v) for n, v in err.items()}
     envm = {n: ranks.max(v) for n, v in envm.items()}
+    compared = {n: int(ranks.sum(v)) for n, v in compared.items()}
     # the same scenarios one at a time through the single-domain path
     step = max(1, len(all_cases) // 32)
 
@@ -290,8 +295,8 @@ def ensemble_leg(args, ranks):
             "mixed_over_solo_fp64": (out["mixed"]["value"] / ranks.world / solo) if solo else None,
             "error_vs_fp64": {"scenarios": [int(k) for k in range(0, len(all_cases), every)][:8],
                               "at_step": cap, "rel_linf": err, "fp32_input_envelope": envm,
-                              "wet_fraction": wet, "empty_fields": sorted(set(empty)),
-                              "valid": not empty and bool(subset)}}
+                              "wet_fraction": wet, "scenarios_compared": compared,
+                              "valid": all(v > 0 for v in compared.values())}}
 
 
 def serving_leg(args):
