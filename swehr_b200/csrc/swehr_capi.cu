@@ -286,12 +286,21 @@ static void stage_part(double *dst, const void *src, size_t n, size_t esize)
 }
 
 /* the host side of a chunk, split over a few threads: filling fresh pageable
- * pages is bound by page faults, which proceed in parallel */
+ * pages is bound by page faults, which proceed in parallel (half the host's
+ * hardware threads, 2..8) */
+static const int kStageThreadsMax = 8;
+
+static int stage_threads()
+{
+    static const int T = std::max(2, std::min(kStageThreadsMax, (int)std::thread::hardware_concurrency() / 2));
+    return T;
+}
+
 static void stage_out(double *dst, const void *src, size_t n, size_t esize)
 {
-    const int T = 4;
+    const int T = stage_threads();
     const size_t per = (n + T - 1) / T;
-    std::thread th[T - 1];
+    std::thread th[kStageThreadsMax - 1];
     for (int t = 1; t < T; t++) {
         const size_t a = std::min(n, (size_t)t * per), b = std::min(n, a + per);
         th[t - 1] = std::thread(stage_part, dst + a, (const char *)src + a * esize, b - a, esize);

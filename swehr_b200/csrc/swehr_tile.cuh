@@ -78,12 +78,30 @@ struct PolicyF64 {
     static __device__ __forceinline__ R cos_atan(R x) { return sw_cos_atan(x); }
     static __device__ __forceinline__ R sin_atan(R x) { return sw_sin_atan(x); }
     static __device__ __forceinline__ R div(R a, R b) { return a / b; }
+    /* a / b where a is often an exact zero: a zero over a positive divisor
+     * is that zero (sign included), so the division sequence is skipped; any
+     * other operands divide as usual (bit-identical to a / b) */
+    static __device__ __forceinline__ R divz(R a, R b)
+    {
+        if (a == 0 && b > 0) return a;
+        return a / b;
+    }
+    /* sqrtp of an argument that is often an exact zero (sqrtp(+-0) = +0) */
+    static __device__ __forceinline__ R sqrtz(R x)
+    {
+        if (x == 0) return R(0);
+        return sqrtp(x);
+    }
     static __device__ __forceinline__ R qnan() { return __longlong_as_double(0x7ff8000000000000LL); }
     /* settling velocity of Cao 2006 (SWEHR.c:435): sqrt(A^2 + c) - A, in the
      * reference's operation order */
     static __device__ __forceinline__ R settle(R A, R A2, R c) { return sqrtp(A2 + c) - A; }
     /* deposited thickness of a deposited mass, DEP += M_k / rhos (SWEHR.c:1510) */
-    static __device__ __forceinline__ double dep_of(double M, const DevParams &P) { return M / P.rhos; }
+    static __device__ __forceinline__ double dep_of(double M, const DevParams &P)
+    {
+        if (M == 0 && P.rhos > 0) return M;
+        return M / P.rhos;
+    }
 };
 
 struct PolicyF32 {
@@ -122,6 +140,8 @@ struct PolicyF32 {
     static __device__ __forceinline__ R cos_atan(R x) { return rsqrtf(1.f + x * x); }
     static __device__ __forceinline__ R sin_atan(R x) { return x * rsqrtf(1.f + x * x); }
     static __device__ __forceinline__ R div(R a, R b) { return __fdividef(a, b); }
+    static __device__ __forceinline__ R divz(R a, R b) { return div(a, b); }
+    static __device__ __forceinline__ R sqrtz(R x) { return sqrtp(x); }
     static __device__ __forceinline__ R qnan() { return __int_as_float(0x7fc00000); }
     /* settling velocity sqrt(A^2 + c) - A rewritten as c / (sqrt(A^2 + c) + A):
      * equal in exact arithmetic, but for fine classes (d = 2 um: A = 8.37,
@@ -144,9 +164,9 @@ __device__ __forceinline__ typename PP::R hllc_v(typename PP::R hl, typename PP:
     const R half = R(0.5);
     const R cr = PP::sqrtp(g * hr);
     const R d = nl + 2 * cl - nr - 2 * cr;
-    const R hs = PP::div(d * d, 16 * g);
+    const R hs = PP::divz(d * d, 16 * g);
     const R us = half * (nl + nr) + cl - cr;
-    const R cs = PP::sqrtp(g * hs);
+    const R cs = PP::sqrtz(g * hs);
     R sl = nl - cl;
     if (us - cs < sl) sl = us - cs;
     R sm = us;
@@ -160,7 +180,7 @@ __device__ __forceinline__ typename PP::R hllc_v(typename PP::R hl, typename PP:
         f1 = hl * nl * nl + half * g * hl * hl;
     }
     if (sl <= 0 && sr >= 0) {
-        f0 = PP::div(sr * (hl * nl) - sl * (hr * nr) + sl * sr * (hr - hl), sr - sl);
+        f0 = PP::divz(sr * (hl * nl) - sl * (hr * nr) + sl * sr * (hr - hl), sr - sl);
         f1 = PP::div(sr * (hl * nl * nl + half * g * hl * hl) - sl * (hr * nr * nr + half * g * hr * hr)
                          + sl * sr * (hr * nr - hl * nl),
                      sr - sl);
@@ -198,9 +218,9 @@ __device__ __forceinline__ typename PP::R hll_speed(typename PP::R hl, typename 
     typedef typename PP::R R;
     const R cr = PP::sqrtp(g * hr);
     const R d = nl + 2 * cl - nr - 2 * cr;
-    const R hs = PP::div(d * d, 16 * g);
+    const R hs = PP::divz(d * d, 16 * g);
     const R us = R(0.5) * (nl + nr) + cl - cr;
-    const R cs = PP::sqrtp(g * hs);
+    const R cs = PP::sqrtz(g * hs);
     R sl = nl - cl;
     if (us - cs < sl) sl = us - cs;
     R sm = us;
@@ -888,7 +908,7 @@ __device__ __forceinline__ void tile_cell(const DevParams &P, const SetV<RS> &sr
         depthfac = PP::pow(PP::div(K.h0, hvert), K.b);
         mtstar = K.mtstar0 * depthfac;
     }
-    const R Hs = fmin(one, PP::div(totm0, mtstar));
+    const R Hs = fmin(one, PP::divz(totm0, mtstar));
     const bool swash = (h0v > K.hfx10 && totsed0 < R(0.6));
     R E3b = 0, E4b = 0, e4den = 1;
     if (swash) {
@@ -1004,7 +1024,7 @@ __device__ __forceinline__ void tile_cell(const DevParams &P, const SetV<RS> &sr
                 dep = 0;
             }
         }
-        const R dh = PP::div(u - chtemp, K.porod);
+        const R dh = PP::divz(u - chtemp, K.porod);
         h = h + dh;
         bulk += dh;
         totm += Mk;
@@ -1013,7 +1033,10 @@ __device__ __forceinline__ void tile_cell(const DevParams &P, const SetV<RS> &sr
             Uslot[k * (HALO_ROWS * R_J)] = (RS)u;
         else
             Ureg[kSlot ? 0 : k] = u;
-        dst.M[qm] = Mk;
+        if (L.stage_m)         /* the cell's own staged slot: read back below, no global round trip */
+            const_cast<double *>(celld)[(CD_M + k) * T_I * T_J + cs] = Mk;
+        else
+            dst.M[qm] = Mk;
         if (BUDGET) {
             /* U_k + M_k changes only by the face fluxes and detachment; what
              * the arithmetic and storage add on top is accounted as rounding */
@@ -1034,6 +1057,7 @@ __device__ __forceinline__ void tile_cell(const DevParams &P, const SetV<RS> &sr
             const R uk = kSlot ? (R)Uslot[k * (HALO_ROWS * R_J)] : Ureg[kSlot ? 0 : k];
             totsed += PP::div(PP::div(uk, h), rhos);
             dst.U[k * pl + q] = (RS)uk;
+            if (L.stage_m) dst.M[k * pl + q] = celld[(CD_M + k) * T_I * T_J + cs];
         }
     } else {
         clamp = hfilm - h;
@@ -1046,7 +1070,8 @@ __device__ __forceinline__ void tile_cell(const DevParams &P, const SetV<RS> &sr
             const int64_t qm = k * pl + q;
             const R uk = kSlot ? (R)Uslot[k * (HALO_ROWS * R_J)] : Ureg[kSlot ? 0 : k];
             z = z + P.invporo * (double)uk;
-            dst.M[qm] = dst.M[qm] + (double)uk;
+            const double mk = L.stage_m ? celld[(CD_M + k) * T_I * T_J + cs] : dst.M[qm];
+            dst.M[qm] = mk + (double)uk;
             dst.U[qm] = (RS)0;
         }
     }
@@ -1061,7 +1086,7 @@ __device__ __forceinline__ void tile_cell(const DevParams &P, const SetV<RS> &sr
         vel2 = PP::div(hv, h);
     }
     R maxvel = (R)cellr[CR_MAXVEL * T_I * T_J + cs], maxdep = (R)cellr[CR_MAXDEP * T_I * T_J + cs];
-    const R vmag = PP::sqrtp(vel1 * vel1 + vel2 * vel2);
+    const R vmag = PP::sqrtz(vel1 * vel1 + vel2 * vel2);
     if (vmag > maxvel) maxvel = vmag;
     if (h > maxdep) maxdep = h;
     dst.h[q] = (RS)h;
