@@ -93,6 +93,8 @@ struct Ctl {
     double rain_now;                        /* uniform rain rate of the current / last step */
     double t_prev;                          /* start time of the last completed step */
     double sed0[16];
+    int32_t dev_error;                      /* a bounded device-side wait gave up (SWEHR_TIMEOUT) */
+    int32_t pad_err;
 };
 
 /* budget term slots */

@@ -3,6 +3,7 @@
 #include <cuda_runtime.h>
 
 #include "swehr_device.cuh"
+#include "swehr_tma.cuh"
 
 namespace swehr {
 
@@ -82,6 +83,7 @@ struct StepConfig {
     size_t smem_wave = 0, smem_update = 0;
     void *fn_update = nullptr, *fn_wave = nullptr;
     int stage_m = 1;                    /* the update stages M_k in shared memory */
+    int tma = 0;                        /* in: tensor maps exist (FP64); out: the update loads tiles through them */
 };
 
 /* Pick the kernel instantiations, set their shared-memory limit and size the
@@ -92,14 +94,20 @@ int configure_step_f32(const DevParams &P, int num_sms, StepConfig &cfg);
 /* Enqueue one full step (wave pass + update pass); ev0/ev1 (optional) are
  * recorded around the update kernel. */
 int launch_step_f64(const DevParams &P, const BufsT<double> &B, Ctl *ctl, const double *rain, double *partials,
-                    double *stage, double *saveflow, const StepConfig &cfg, cudaStream_t s, cudaEvent_t ev0,
-                    cudaEvent_t ev1);
+                    double *stage, double *saveflow, const TmaMaps &tm, const StepConfig &cfg, cudaStream_t s,
+                    cudaEvent_t ev0, cudaEvent_t ev1);
+/* the update kernel's tile loads through tensor maps (FP64 form, one
+ * domain): whether the driver offers the encoder, and the maps of a
+ * simulation's planes (0 when all were encoded) */
+int tma_available_f64();
+int encode_tma_f64(const DevParams &P, const BufsT<double> &B, TmaMaps &tm);
+
 /* the gz plane of the set step n reads, from its previous-step topography
  * (at creation and after the topography is written) */
 int init_gz_f64(const DevParams &P, const BufsT<double> &B, int64_t n, cudaStream_t s);
 int init_gz_f32(const DevParams &P, const BufsT<float> &B, int64_t n, cudaStream_t s);
 int launch_step_f32(const DevParams &P, const BufsT<float> &B, Ctl *ctl, const double *rain, double *partials,
-                    double *stage, double *saveflow, const StepConfig &cfg, cudaStream_t s, cudaEvent_t ev0,
-                    cudaEvent_t ev1);
+                    double *stage, double *saveflow, const TmaMaps &tm, const StepConfig &cfg, cudaStream_t s,
+                    cudaEvent_t ev0, cudaEvent_t ev1);
 
 }  // namespace swehr

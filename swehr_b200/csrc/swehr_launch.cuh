@@ -6,6 +6,8 @@
 #pragma once
 #include <cuda_runtime.h>
 
+#include <type_traits>
+
 #include "swehr_kernels.h"
 #include "swehr_tile.cuh"
 
@@ -24,9 +26,9 @@ struct FormLauncher {
      * doubles the resident blocks and the update runs ~27 % faster).  Sets
      * both kernels' shared-memory limits. */
     static cudaError_t pick_staging(void *f_with, void *f_without, int S, size_t &smem, int &occ, int &stage_m,
-                                    void *&fn)
+                                    void *&fn, size_t extra = 0)
     {
-        const size_t with = update_smem(S, 1), without = update_smem(S, 0);
+        const size_t with = update_smem(S, 1) + extra, without = update_smem(S, 0) + extra;
         int ow = 0, oo = 0;
         cudaError_t e = cudaFuncSetAttribute(f_with, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)with);
         if (e != cudaSuccess) return e;
@@ -51,21 +53,34 @@ struct FormLauncher {
         return (int)cudaGetLastError();
     }
 
-    template <int MAXS, bool BUDGET, bool SM>
-    static void *update_fn() { return (void *)k_update_tile<PP, RS, MAXS, BUDGET, SM>; }
+    /* tile loads through tensor maps exist for the FP64 form (its planes'
+     * staged windows start on 16-byte columns) */
+    static constexpr bool kHasTma = std::is_same<RS, double>::value;
 
-    template <bool BUDGET, bool SM>
+    template <int MAXS, bool BUDGET, bool SM, bool TMA>
+    static void *update_fn() { return (void *)k_update_tile<PP, RS, MAXS, BUDGET, SM, TMA>; }
+
+    template <bool BUDGET, bool SM, bool TMA>
     static void *pick_u(int S)
     {
-        if (S <= 4) return update_fn<4, BUDGET, SM>();
-        if (S <= 8) return update_fn<8, BUDGET, SM>();
-        return update_fn<16, BUDGET, SM>();
+        if (S <= 4) return update_fn<4, BUDGET, SM, TMA>();
+        if (S <= 8) return update_fn<8, BUDGET, SM, TMA>();
+        return update_fn<16, BUDGET, SM, TMA>();
     }
 
-    static void *pick_update(int S, bool budget, bool sm)
+    template <bool TMA>
+    static void *pick_update_t(int S, bool budget, bool sm)
     {
-        if (budget) return sm ? pick_u<true, true>(S) : pick_u<true, false>(S);
-        return sm ? pick_u<false, true>(S) : pick_u<false, false>(S);
+        if (budget) return sm ? pick_u<true, true, TMA>(S) : pick_u<true, false, TMA>(S);
+        return sm ? pick_u<false, true, TMA>(S) : pick_u<false, false, TMA>(S);
+    }
+
+    static void *pick_update(int S, bool budget, bool sm, bool tma = false)
+    {
+        if constexpr (kHasTma) {
+            if (tma) return pick_update_t<true>(S, budget, sm);
+        }
+        return pick_update_t<false>(S, budget, sm);
     }
 
     static int configure(const DevParams &P, int num_sms, StepConfig &cfg)
@@ -76,8 +91,11 @@ struct FormLauncher {
         size_t su = 0;
         const size_t sw = wave_smem();
         int occ_u = 0, occ_w = 0, stage_m = 1;
-        cudaError_t e = pick_staging(pick_update(P.S, P.budget != 0, true), pick_update(P.S, P.budget != 0, false),
-                                     P.S, su, occ_u, stage_m, fu);
+        const bool tma = kHasTma && cfg.tma;
+        cfg.tma = tma ? 1 : 0;
+        cudaError_t e = pick_staging(pick_update(P.S, P.budget != 0, true, tma),
+                                     pick_update(P.S, P.budget != 0, false, tma), P.S, su, occ_u, stage_m, fu,
+                                     tma ? 128 : 0);
         if (e != cudaSuccess) return (int)e;
         e = cudaFuncSetAttribute(fw, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sw);
         if (e != cudaSuccess) return (int)e;
@@ -140,14 +158,14 @@ struct FormLauncher {
     }
 
     static int launch(const DevParams &P, const BufsT<RS> &B, Ctl *ctl, const double *rain, double *partials,
-                      double *stage, double *saveflow, const StepConfig &cfg, cudaStream_t s, cudaEvent_t ev0,
-                      cudaEvent_t ev1)
+                      double *stage, double *saveflow, const TmaMaps &tm, const StepConfig &cfg, cudaStream_t s,
+                      cudaEvent_t ev0, cudaEvent_t ev1)
     {
         void *wargs[] = {(void *)&P, (void *)&B, (void *)&ctl};
         cudaLaunchKernel(cfg.fn_wave, dim3(cfg.grid_wave), dim3(TILE_THREADS), wargs, cfg.smem_wave, s);
         if (ev0) cudaEventRecord(ev0, s);
         void *args[] = {(void *)&P, (void *)&B, (void *)&ctl, (void *)&rain, (void *)&partials, (void *)&stage,
-                        (void *)&saveflow};
+                        (void *)&saveflow, (void *)&tm};
         cudaLaunchKernel(cfg.fn_update, dim3(cfg.grid_update), dim3(TILE_THREADS), args, cfg.smem_update, s);
         if (ev1) cudaEventRecord(ev1, s);
         return (int)cudaGetLastError();

@@ -20,10 +20,10 @@ int init_gz_f32(const DevParams &P, const BufsT<float> &B, int64_t n, cudaStream
 }
 
 int launch_step_f32(const DevParams &P, const BufsT<float> &B, Ctl *ctl, const double *rain, double *partials,
-                    double *stage, double *saveflow, const StepConfig &cfg, cudaStream_t s, cudaEvent_t ev0,
-                    cudaEvent_t ev1)
+                    double *stage, double *saveflow, const TmaMaps &tm, const StepConfig &cfg, cudaStream_t s,
+                    cudaEvent_t ev0, cudaEvent_t ev1)
 {
-    return FormLauncher<PolicyF32, float>::launch(P, B, ctl, rain, partials, stage, saveflow, cfg, s, ev0, ev1);
+    return FormLauncher<PolicyF32, float>::launch(P, B, ctl, rain, partials, stage, saveflow, tm, cfg, s, ev0, ev1);
 }
 
 int configure_batch_f32(int max_classes, bool budget, BatchConfig &cfg)

@@ -32,6 +32,7 @@
 #include "swehr_device.cuh"
 #include "swehr_faces.cuh"
 #include "swehr_kernels.h"
+#include "swehr_tma.cuh"
 
 #include <cuda_pipeline_primitives.h>
 
@@ -272,6 +273,7 @@ struct StagedLayout {
     /* byte offsets from the start of dynamic shared memory */
     size_t halo, cell_r, cell_d, zp, zc, u, v, g, c, sed, fx, fy, up, red, total;
     int nhalo, ncellr, ncelld;
+    int hps;              /* elements from one halo plane to the next (rows x R_J, rounded to 128 bytes) */
     int stage_m;          /* M_k staged here (else read from global memory by the cell stage) */
     /* stage_m: staging M_k costs 2 KB of shared memory per class; the
      * launcher picks the kernel that stages it only where that costs no
@@ -280,12 +282,14 @@ struct StagedLayout {
     {
         StagedLayout L;
         size_t o = 0;
-        auto take = [&](size_t bytes) { size_t at = o; o += (bytes + 15) / 16 * 16; return at; };
+        /* every region starts 128-byte aligned (a tile copy's destination) */
+        auto take = [&](size_t bytes) { size_t at = o; o += (bytes + 127) / 128 * 128; return at; };
+        L.hps = (int)(((size_t)HALO_ROWS * R_J * rs + 127) / 128 * 128 / rs);
         L.stage_m = stage_m;
         L.nhalo = 5 + S;
         L.ncellr = 4;
         L.ncelld = L.stage_m ? 1 + S : 1;
-        L.halo = take((size_t)L.nhalo * HALO_ROWS * R_J * rs);
+        L.halo = take((size_t)L.nhalo * L.hps * rs);
         L.cell_r = take((size_t)L.ncellr * T_I * T_J * rs);
         L.cell_d = take((size_t)L.ncelld * T_I * T_J * sizeof(double));
         L.zp = take((size_t)ZP_ROWS * R_J * sizeof(double));
@@ -352,7 +356,7 @@ __device__ __forceinline__ void stage_load(const DevParams &P, const SetV<RS> &s
         if (gi >= 1 && gi <= P.nx && col >= 0 && col < P.ny) {
             const int64_t go = (int64_t)(gi - 1) * P.pitch + col;
             RS *d = reinterpret_cast<RS *>(smb + L.halo) + r * R_J + 2 * k2;
-            const int ps = HALO_ROWS * R_J;
+            const int ps = L.hps;
             cp_pair(d + HP_H * ps, src.h + go);
             cp_pair(d + HP_HU * ps, src.hu + go);
             cp_pair(d + HP_HV * ps, src.hv + go);
@@ -398,6 +402,43 @@ __device__ __forceinline__ void stage_load(const DevParams &P, const SetV<RS> &s
         }
     }
     __pipeline_commit();
+}
+
+/* The same staging as stage_load as tensor-map box copies (FP64 planes of
+ * one domain), issued by one thread onto the tile's mbarrier: halo boxes
+ * R_J x halo rows at column j0-3, row i0-2 (0-based), the z_prev window one
+ * row higher and taller, cell boxes T_J x T_I at (j0-1, i0-1).  x = j0-3 is
+ * even, so every box starts on a 16-byte column boundary; rows or columns
+ * outside the grid arrive as zeros. */
+__device__ __forceinline__ void stage_load_tma(const DevParams &P, const TmaMaps &tm, int set, int64_t n,
+                                               TileCoord tc, unsigned char *smb, const StagedLayout &L,
+                                               uint64_t *bar)
+{
+    const uint32_t hb = (uint32_t)(HALO_ROWS * R_J * sizeof(double));
+    const uint32_t cb = (uint32_t)(T_I * T_J * sizeof(double));
+    const uint32_t bytes = (uint32_t)(5 + P.S) * hb + (uint32_t)((ZP_ROWS + ZC_ROWS) * R_J * sizeof(double)) +
+                           (3u + (P.has_ks ? 1u : 0u) + 1u + (L.stage_m ? (uint32_t)P.S : 0u)) * cb;
+    mbar_expect_tx(bar, bytes);
+    const CUtensorMap *mh = &tm.m[TM_HALO0 + set], *mc = &tm.m[TM_CELL0 + set];
+    const int hx = tc.j0 - 3, hy = tc.i0 - 2, cx = tc.j0 - 1, cy = tc.i0 - 1;
+    double *halo = reinterpret_cast<double *>(smb + L.halo);
+    tma_load_3d(halo + HP_H * L.hps, mh, bar, hx, hy, P_H);
+    tma_load_3d(halo + HP_HU * L.hps, mh, bar, hx, hy, P_HU);
+    tma_load_3d(halo + HP_HV * L.hps, mh, bar, hx, hy, P_HV);
+    tma_load_3d(halo + HP_TS * L.hps, mh, bar, hx, hy, P_TOTSED);
+    tma_load_3d(halo + HP_DEP * L.hps, mh, bar, hx, hy, P_DEP);
+    for (int k = 0; k < P.S; k++) tma_load_3d(halo + (HP_U + k) * L.hps, mh, bar, hx, hy, P_FIXED + k);
+    tma_load_3d(smb + L.zp, &tm.m[TM_ZP], bar, hx, tc.i0 - 3, (int)((n + 2) % 3));
+    tma_load_3d(smb + L.zc, &tm.m[TM_ZC], bar, hx, hy, (int)(n % 3));
+    double *cr = reinterpret_cast<double *>(smb + L.cell_r), *cd = reinterpret_cast<double *>(smb + L.cell_d);
+    const int ps = T_I * T_J;
+    tma_load_3d(cr + CR_TOTM * ps, mc, bar, cx, cy, P_TOTM);
+    tma_load_3d(cr + CR_MAXVEL * ps, mc, bar, cx, cy, P_MAXVEL);
+    tma_load_3d(cr + CR_MAXDEP * ps, mc, bar, cx, cy, P_MAXDEP);
+    if (P.has_ks) tma_load_3d(cr + CR_KS * ps, &tm.m[TM_KS], bar, cx, cy, 0);
+    tma_load_3d(cd + CD_VINF * ps, mc, bar, cx, cy, P_VINF);
+    if (L.stage_m)
+        for (int k = 0; k < P.S; k++) tma_load_3d(cd + (CD_M + k) * ps, mc, bar, cx, cy, P_FIXED + P.S + k);
 }
 
 /* slopes from a staged topography tile, same operations as slope_x/slope_y
@@ -446,9 +487,9 @@ __device__ __forceinline__ void stage_derive(const DevParams &P, const SetV<RS> 
         if (inflow) {
             h = inh; hu = 0; hv = inhv;
         } else {
-            h = (R)halo[(HP_H * HALO_ROWS) * R_J + so];
-            hu = (R)halo[(HP_HU * HALO_ROWS) * R_J + so];
-            hv = (R)halo[(HP_HV * HALO_ROWS) * R_J + so];
+            h = (R)halo[HP_H * L.hps + so];
+            hu = (R)halo[HP_HU * L.hps + so];
+            hv = (R)halo[HP_HV * L.hps + so];
             if ((gi == 0 && P.bndry[0] == 1) || (gi == P.nx + 1 && P.bndry[2] == 1)) hu = -hu;
             if ((gj == 0 && P.bndry[1] == 1) || (gj == P.ny + 1 && P.bndry[3] == 1)) hv = -hv;
         }
@@ -456,7 +497,7 @@ __device__ __forceinline__ void stage_derive(const DevParams &P, const SetV<RS> 
         if (h > K.hfilm) { u = PP::div(hu, h); v = PP::div(hv, h); }
         if (gx || gy) {
             /* ghost cells are never read through the staged planes: keep h there */
-            reinterpret_cast<RS *>(smb + L.halo)[(HP_H * HALO_ROWS + hi) * R_J + hj + 1] = (RS)h;
+            reinterpret_cast<RS *>(smb + L.halo)[HP_H * L.hps + hi * R_J + hj + 1] = (RS)h;
         }
         su[idx] = u;
         sv[idx] = v;
@@ -479,7 +520,7 @@ __device__ __forceinline__ void stage_derive(const DevParams &P, const SetV<RS> 
             R s = 0;
             if (inflow) s = insed;
             else if (h > K.hfilm) {
-                s = PP::div((R)halo[((HP_U + k) * HALO_ROWS) * R_J + so], h);
+                s = PP::div((R)halo[(HP_U + k) * L.hps + so], h);
                 if (s < R(-1e-5)) s = 0;
             }
             ssed[k * N_H + idx] = s;
@@ -497,7 +538,7 @@ __device__ __forceinline__ void stage_derive(const DevParams &P, const SetV<RS> 
 template <class RS>
 __device__ __forceinline__ const RS *staged_h(const unsigned char *smb, const StagedLayout &L)
 {
-    return reinterpret_cast<const RS *>(smb + L.halo) + (HP_H * HALO_ROWS) * R_J;
+    return reinterpret_cast<const RS *>(smb + L.halo) + HP_H * L.hps;
 }
 
 /* ------------------------------------------------------------------ wave */
@@ -826,9 +867,9 @@ __device__ __forceinline__ void tile_cell(const DevParams &P, const SetV<RS> &sr
     const RS *halo = reinterpret_cast<const RS *>(smb + L.halo);
     const RS *cellr = reinterpret_cast<const RS *>(smb + L.cell_r);
     const double *celld = reinterpret_cast<const double *>(smb + L.cell_d);
-    const RS *sTS = halo + (HP_TS * HALO_ROWS) * R_J, *sDEP = halo + (HP_DEP * HALO_ROWS) * R_J;
-    const R h0v = (R)halo[(HP_H * HALO_ROWS) * R_J + so];
-    const R hu0 = (R)halo[(HP_HU * HALO_ROWS) * R_J + so], hv0 = (R)halo[(HP_HV * HALO_ROWS) * R_J + so];
+    const RS *sTS = halo + HP_TS * L.hps, *sDEP = halo + HP_DEP * L.hps;
+    const R h0v = (R)halo[HP_H * L.hps + so];
+    const R hu0 = (R)halo[HP_HU * L.hps + so], hv0 = (R)halo[HP_HV * L.hps + so];
     const R totsed0 = (R)sTS[so], dep0 = (R)sDEP[so];
     const R totm0 = (R)cellr[CR_TOTM * T_I * T_J + cs];
     R rho0c = rhow * (1 - totsed0) + rhos * totsed0;
@@ -948,14 +989,15 @@ __device__ __forceinline__ void tile_cell(const DevParams &P, const SetV<RS> &sr
     constexpr bool kSlot = PP::kRollClasses;
     static_assert(sizeof(R) == sizeof(RS), "the staged U_k slot holds a U_k value");
     const R *SED = reinterpret_cast<const R *>(smb + L.sed);
-    RS *Uslot = reinterpret_cast<RS *>(const_cast<unsigned char *>(smb) + L.halo) + (HP_U * HALO_ROWS) * R_J + so;
+    RS *Uslot = reinterpret_cast<RS *>(const_cast<unsigned char *>(smb) + L.halo) + HP_U * L.hps + so;
+    const int hps = L.hps;
     R Ureg[kSlot ? 1 : MAXS];
     if constexpr (!kSlot) {
 #pragma unroll
         for (int k = 0; k < MAXS; k++) {
             if (k >= S) break;
             const R *sk = SED + k * N_H;
-            Ureg[k] = (R)Uslot[k * (HALO_ROWS * R_J)] - dtdx * (fxr0 * sk[uxr] - fxl0 * sk[uxl])
+            Ureg[k] = (R)Uslot[k * hps] - dtdx * (fxr0 * sk[uxr] - fxl0 * sk[uxl])
                       - dtdx * (fyr0 * sk[uyr] - fyl0 * sk[uyl]);
         }
     }
@@ -967,7 +1009,7 @@ __device__ __forceinline__ void tile_cell(const DevParams &P, const SetV<RS> &sr
         if (k >= S) break;
         const int64_t qm = k * pl + q;
         const R *sk = SED + k * N_H;
-        const RS u_in = Uslot[k * (HALO_ROWS * R_J)];
+        const RS u_in = Uslot[k * hps];
         R uflux;
         if constexpr (kSlot)
             uflux = (R)u_in - dtdx * (fxr0 * sk[uxr] - fxl0 * sk[uxl]) - dtdx * (fyr0 * sk[uyr] - fyl0 * sk[uyl]);
@@ -1030,7 +1072,7 @@ __device__ __forceinline__ void tile_cell(const DevParams &P, const SetV<RS> &sr
         totm += Mk;
         dep += PP::dep_of(Mk, P);
         if constexpr (kSlot)
-            Uslot[k * (HALO_ROWS * R_J)] = (RS)u;
+            Uslot[k * hps] = (RS)u;
         else
             Ureg[kSlot ? 0 : k] = u;
         if (L.stage_m)         /* the cell's own staged slot: read back below, no global round trip */
@@ -1054,7 +1096,7 @@ __device__ __forceinline__ void tile_cell(const DevParams &P, const SetV<RS> &sr
 #pragma unroll
         for (int k = 0; k < MAXS; k++) {
             if (k >= S) break;
-            const R uk = kSlot ? (R)Uslot[k * (HALO_ROWS * R_J)] : Ureg[kSlot ? 0 : k];
+            const R uk = kSlot ? (R)Uslot[k * hps] : Ureg[kSlot ? 0 : k];
             totsed += PP::div(PP::div(uk, h), rhos);
             dst.U[k * pl + q] = (RS)uk;
             if (L.stage_m) dst.M[k * pl + q] = celld[(CD_M + k) * T_I * T_J + cs];
@@ -1068,7 +1110,7 @@ __device__ __forceinline__ void tile_cell(const DevParams &P, const SetV<RS> &sr
         for (int k = 0; k < MAXS; k++) {
             if (k >= S) break;
             const int64_t qm = k * pl + q;
-            const R uk = kSlot ? (R)Uslot[k * (HALO_ROWS * R_J)] : Ureg[kSlot ? 0 : k];
+            const R uk = kSlot ? (R)Uslot[k * hps] : Ureg[kSlot ? 0 : k];
             z = z + P.invporo * (double)uk;
             const double mk = L.stage_m ? celld[(CD_M + k) * T_I * T_J + cs] : dst.M[qm];
             dst.M[qm] = mk + (double)uk;
@@ -1187,10 +1229,11 @@ __device__ __forceinline__ void stage_sample_tile(const DevParams &P, const SetV
 
 /* Update of one tile: stages A (staging), B (faces), C (cells).  The whole
  * block calls it. */
-template <class PP, class RS, int MAXS, bool BUDGET>
+template <class PP, class RS, int MAXS, bool BUDGET, bool TMA = false>
 __device__ __forceinline__ void update_tile(const DevParams &P, const BufsT<RS> &B, int64_t n, double t, double dt,
                                             double Rr, TileCoord tc, unsigned char *smb, const StagedLayout &L,
-                                            Acc2<MAXS, BUDGET> &acc)
+                                            Acc2<MAXS, BUDGET> &acc, const TmaMaps *tm = nullptr,
+                                            uint64_t *bar = nullptr, uint32_t *phase = nullptr, Ctl *ctl = nullptr)
 {
     typedef typename PP::R R;
     const RealC<R> &K = kc<R>(P);
@@ -1204,9 +1247,21 @@ __device__ __forceinline__ void update_tile(const DevParams &P, const BufsT<RS> 
     const R *su = reinterpret_cast<const R *>(smb + L.u), *sv = reinterpret_cast<const R *>(smb + L.v);
     const R *sg = reinterpret_cast<const R *>(smb + L.g), *sc = reinterpret_cast<const R *>(smb + L.c);
     R *sfx = reinterpret_cast<R *>(smb + L.fx), *sfy = reinterpret_cast<R *>(smb + L.fy);
-    stage_load<RS>(P, src, zp, zc, B.ks, tc, smb, L);
-    __pipeline_wait_prior(0);
-    __syncthreads();
+    if constexpr (TMA) {
+        /* the previous tile's reads and writes of these buffers are done
+         * (the barrier ending it); order them before the copies that land */
+        if (threadIdx.x == 0) {
+            fence_proxy_async_smem();
+            stage_load_tma(P, *tm, (int)(n & 1), n, tc, smb, L, bar);
+        }
+        if (!mbar_wait_bounded(bar, *phase & 1u) && threadIdx.x == 0) ctl->dev_error = 1;
+        *phase += 1;
+        __syncthreads();
+    } else {
+        stage_load<RS>(P, src, zp, zc, B.ks, tc, smb, L);
+        __pipeline_wait_prior(0);
+        __syncthreads();
+    }
     stage_derive<PP, RS>(P, src, tc, smb, L, (R)inh, (R)inhv, (R)insed);
     __syncthreads();
     const RS *sh = staged_h<RS>(smb, L);
@@ -1326,6 +1381,10 @@ __device__ __forceinline__ void update_finalize(const DevParams &P, const SetV<R
         ctl->update_ticket = 0u;
         if (ctl->cfl) ctl->status = 1;
         if (!(dt > 0) && !ctl->cfl) ctl->status = 2;
+        if (ctl->dev_error) {
+            ctl->status = 3;
+            ctl->active = 0;
+        }
         if (ctl->cfl || !(dt > 0) || !(tnew < P.tend) || !(tnew < ctl->t_stop) || n + 1 >= ctl->max_step)
             ctl->active = 0;
         ctl->launches += 2;
@@ -1341,15 +1400,30 @@ __device__ __forceinline__ void budget_fold(Ctl *ctl, int m, double hi, double l
     ctl->budget_lo[m] = Ll;
 }
 
-template <class PP, class RS, int MAXS, bool BUDGET, bool STAGE_M>
+template <class PP, class RS, int MAXS, bool BUDGET, bool STAGE_M, bool TMA>
 __global__ void __launch_bounds__(TILE_THREADS, PP::kMinBlocks) k_update_tile(const DevParams P, const BufsT<RS> B, Ctl *ctl,
                                                                   const double *__restrict__ rain, double *partials,
-                                                                  double *stage, double *saveflow)
+                                                                  double *stage, double *saveflow,
+                                                                  const __grid_constant__ TmaMaps tm)
 {
     typedef typename PP::R R;
     if (!ctl->pending) return;
-    extern __shared__ __align__(16) unsigned char smb[];
+    extern __shared__ __align__(128) unsigned char smb_raw[];
+    /* tile-copy destinations must start on 128 bytes: with tensor-map loads
+     * the launch adds 128 bytes and the staging starts at the next boundary */
+    unsigned char *smb = TMA ? reinterpret_cast<unsigned char *>((reinterpret_cast<uintptr_t>(smb_raw) + 127) &
+                                                                ~static_cast<uintptr_t>(127))
+                             : smb_raw;
     __shared__ bool last;
+    __shared__ __align__(8) uint64_t tma_bar;
+    uint32_t tma_phase = 0;
+    if constexpr (TMA) {
+        if (threadIdx.x == 0) {
+            mbar_init(&tma_bar, 1);
+            mbar_init_fence();
+        }
+        __syncthreads();
+    }
     const StagedLayout L = StagedLayout::make(P.S, sizeof(R), STAGE_M);
     const int64_t n = ctl->step;
     const double t = ctl->t, dt = ctl->dt;
@@ -1358,7 +1432,8 @@ __global__ void __launch_bounds__(TILE_THREADS, PP::kMinBlocks) k_update_tile(co
     acc_zero(acc);
     const int64_t ntiles = (int64_t)((P.nx + T_I - 1) / T_I) * ((P.ny + T_J - 1) / T_J);
     for (int64_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x)
-        update_tile<PP, RS, MAXS, BUDGET>(P, B, n, t, dt, Rr, tile_coord(P, tile), smb, L, acc);
+        update_tile<PP, RS, MAXS, BUDGET, TMA>(P, B, n, t, dt, Rr, tile_coord(P, tile), smb, L, acc, &tm, &tma_bar,
+                                               &tma_phase, ctl);
     double *red = reinterpret_cast<double *>(smb + L.red);
     if (BUDGET) budget_block_sum(acc, red);
     __threadfence();
@@ -1527,7 +1602,7 @@ template <class PP, class RS, int MAXS, bool BUDGET, bool STAGE_M>
 __global__ void __launch_bounds__(TILE_THREADS, PP::kMinBlocks) k_update_batch(const BatchHdr<RS> *__restrict__ hdr)
 {
     typedef typename PP::R R;
-    extern __shared__ __align__(16) unsigned char smb[];
+    extern __shared__ __align__(128) unsigned char smb[];
     __shared__ bool last;
     __shared__ __align__(16) ScenDesc<RS> sd;
     __shared__ StepSnap snap;
