@@ -925,6 +925,43 @@ int orc_threads(void)
 #endif
 }
 
+/* The update kernel's division by a constant c through its correctly rounded
+ * reciprocal yc (two remainder corrections), restated for the test that
+ * checks it against IEEE division on the CPU; same guards as the kernel. */
+double orc_divk(double a, double c, double yc)
+{
+    double aa = fabs(a);
+    if (aa >= 0x1p-900 && aa <= 0x1p900) {
+        double q = a * yc;
+        double r = fma(-c, q, a);
+        q = fma(r, yc, q);
+        r = fma(-c, q, a);
+        return fma(r, yc, q);
+    }
+    if (a == 0 && c > 0) return a;
+    return a / c;
+}
+
+/* count of n pseudo-random dividends (a xorshift stream from seed, spread
+ * over [2^-960, 2^960] with both signs and random significands) whose
+ * orc_divk quotient differs in any bit from a / c */
+int64_t orc_divk_check(double c, int64_t n, uint64_t seed)
+{
+    double yc = 1.0 / c;
+    int64_t bad = 0;
+    uint64_t x = seed ? seed : 88172645463325252ull;
+    for (int64_t k = 0; k < n; k++) {
+        x ^= x << 13; x ^= x >> 7; x ^= x << 17;
+        uint64_t e = 1023 - 960 + (x % 1921);                 /* exponent 2^-960 .. 2^960 */
+        uint64_t bits = ((x >> 11) & 0x000fffffffffffffull) | (e << 52) | ((x & 1) << 63);
+        double a;
+        memcpy(&a, &bits, sizeof a);
+        double q1 = orc_divk(a, c, yc), q2 = a / c;
+        if (memcmp(&q1, &q2, sizeof q1) != 0) bad++;
+    }
+    return bad;
+}
+
 /* Elementary-function entry points for the accuracy tests. */
 double orc_m_pow(double x, double y) { return M_POW(x, y); }
 double orc_m_powh(double x) { return M_POWH(x); }

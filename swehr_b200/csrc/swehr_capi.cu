@@ -232,6 +232,15 @@ static void make_devparams(const swehr_params *p, const swehr_inputs *in, const 
     P.c109s = 1.09 * (p->rhos / p->rhow - 1);
     P.rhos08 = 0.8 * p->rhos;
     P.inv_rhos = 1.0 / p->rhos;
+    P.inv_J = 1.0 / p->J;
+    P.inv_h0x6 = 1.0 / P.h0x6;
+    P.inv_p2 = 1.0 / 0.2;
+    P.inv_dtheta = 1.0 / (p->thetas - p->theta0);
+    {
+        auto in_range = [](double c) { return c >= 0x1p-100 && c <= 0x1p100; };
+        P.divk_ok = in_range(P.porod) && in_range(p->rhos) && in_range(p->J) && in_range(P.h0x6) &&
+                    in_range(p->thetas - p->theta0);
+    }
     P.storm_peak = p->storm_peak; P.storm_r2 = p->storm_radius * p->storm_radius;
     P.storm_x0 = p->storm_x0; P.storm_y0 = p->storm_y0; P.storm_vx = p->storm_vx; P.storm_vy = p->storm_vy;
     for (int k = 0; k < p->sclass; k++) {

@@ -52,6 +52,11 @@ struct DevParams {
     double c109s;         /* 1.09*(rhos/rhow-1), settlingvelocity (SWEHR.c:433-435) */
     double rhos08;        /* 0.8*rhos */
     double inv_rhos;      /* 1/rhos (the mixed form's deposited thickness) */
+    /* correctly rounded reciprocals of the constant divisors J, 6 h0, 0.2 and
+     * thetas - theta0, for exact division by remainder correction (divk);
+     * divk_ok: every constant divisor lies in [2^-100, 2^100] */
+    double inv_J, inv_h0x6, inv_p2, inv_dtheta;
+    int32_t divk_ok, pad_divk;
     double storm_peak, storm_r2, storm_x0, storm_y0, storm_vx, storm_vy;
     double ds[16], pf[16], a13[16], a13sq[16];
     RealC<double> kd;     /* the constants above, for templated kernels */

@@ -94,14 +94,36 @@ struct PolicyF64 {
         return sqrtp(x);
     }
     static __device__ __forceinline__ R qnan() { return __longlong_as_double(0x7ff8000000000000LL); }
+    /* a / c for a constant divisor c in [2^-100, 2^100] whose correctly
+     * rounded reciprocal yc the host computed, without the division
+     * sequence: q0 = a yc, then two remainder corrections (Markstein).  The
+     * first leaves q within one ulp of a/c (a faithful quotient), so the
+     * second remainder a - c q is exact and q + r yc rounds to the correctly
+     * rounded a/c (Markstein's theorem for a reciprocal within half an ulp).
+     * Taken only for |a| in [2^-900, 2^900], where no step under- or
+     * overflows; a zero over the positive c is that zero; anything else, or
+     * a launch whose constants are out of range (ok = 0), divides as usual.
+     * The result is the IEEE quotient a / c in every case. */
+    static __device__ __forceinline__ R divk(R a, R c, R yc, int ok)
+    {
+        const R aa = fabs(a);
+        if (ok && aa >= 0x1p-900 && aa <= 0x1p900) {
+            R q = a * yc;
+            R r = fma(-c, q, a);
+            q = fma(r, yc, q);
+            r = fma(-c, q, a);
+            return fma(r, yc, q);
+        }
+        if (a == 0 && c > 0) return a;
+        return a / c;
+    }
     /* settling velocity of Cao 2006 (SWEHR.c:435): sqrt(A^2 + c) - A, in the
      * reference's operation order */
     static __device__ __forceinline__ R settle(R A, R A2, R c) { return sqrtp(A2 + c) - A; }
     /* deposited thickness of a deposited mass, DEP += M_k / rhos (SWEHR.c:1510) */
     static __device__ __forceinline__ double dep_of(double M, const DevParams &P)
     {
-        if (M == 0 && P.rhos > 0) return M;
-        return M / P.rhos;
+        return divk(M, P.rhos, P.inv_rhos, P.divk_ok);
     }
 };
 
@@ -143,6 +165,7 @@ struct PolicyF32 {
     static __device__ __forceinline__ R div(R a, R b) { return __fdividef(a, b); }
     static __device__ __forceinline__ R divz(R a, R b) { return div(a, b); }
     static __device__ __forceinline__ R sqrtz(R x) { return sqrtp(x); }
+    static __device__ __forceinline__ R divk(R a, R c, R, int) { return div(a, c); }
     static __device__ __forceinline__ R qnan() { return __int_as_float(0x7fc00000); }
     /* settling velocity sqrt(A^2 + c) - A rewritten as c / (sqrt(A^2 + c) + A):
      * equal in exact arithmetic, but for fine classes (d = 2 um: A = 8.37,
@@ -933,7 +956,7 @@ __device__ __forceinline__ void tile_cell(const DevParams &P, const SetV<RS> &sr
             fail = fail_exact<PP, RS>(fa, src.dep, zp, zc, i, j, sx, sy, gz, dep0, rho0c, h0v);
         }
     }
-    R dfmask = fmin(one, PP::div(totsed0 - R(0.2), R(0.2)));
+    R dfmask = fmin(one, PP::divk(totsed0 - R(0.2), R(0.2), (R)P.inv_p2, P.divk_ok));
     if (h0v < K.h0x9 || totsed0 < R(0.2)) dfmask = 0;
     R betax = K.neg1ml * gz * h0v * K.fa;
     R betay = K.neg1ml * gz * h0v * K.fa;
@@ -961,7 +984,7 @@ __device__ __forceinline__ void tile_cell(const DevParams &P, const SetV<RS> &sr
         const R omega = rho0c * gz * SF * qq;
         if (omega > K.uc && totsed0 < R(0.6)) E3b = K.af * (omega - K.uc);
         if (omega > K.uc2 && totsed0 < R(0.6)) E4b = K.afr * (omega - K.uc2);
-        e4den = PP::div(rhos - rho0c, rhos) * gz * h0v;
+        e4den = PP::divk(rhos - rho0c, rhos, (R)P.inv_rhos, P.divk_ok) * gz * h0v;
     }
     const R vfconc = PP::pow(1 - fmin(totsed0, R(0.99)), R(4.0));
     const bool debris = (h0v > K.h0x9 && totsed0 > K.cthreshold);
@@ -974,7 +997,7 @@ __device__ __forceinline__ void tile_cell(const DevParams &P, const SetV<RS> &sr
     /* Green-Ampt in FP64 (SWEHR.c:1449-1452) */
     const double ks = P.has_ks ? (double)cellr[CR_KS * T_I * T_J + cs] : P.ks;
     const double vinf0 = celld[CD_VINF * T_I * T_J + cs];
-    const double zf = vinf0 / (P.thetas - P.theta0);
+    const double zf = PolicyF64::divk(vinf0, P.thetas - P.theta0, P.inv_dtheta, P.divk_ok);
     const double hd = (double)h;
     const double infl = fmin(hd - P.hfilm, dt * ks * (zf + P.hf + hd) / zf);
     const double vinf = vinf0 + infl;
@@ -1039,15 +1062,17 @@ __device__ __forceinline__ void tile_cell(const DevParams &P, const SetV<RS> &sr
             if (swash && !debris) {
                 if (totm0 > R(1e-8) && Mk0r > R(1e-8)) E2 = PP::div(Hs * Mk0r, totm0) * K.ad * Rc;
                 if (deepv) E2 = E2 * depthfac;
-                E3 = PP::div((1 - Hs) * K.pf[k] * K.F, K.J) * (h0v > K.ds[k] ? E3b : R(0));
+                E3 = PP::divk((1 - Hs) * K.pf[k] * K.F, K.J, (R)P.inv_J, P.divk_ok) * (h0v > K.ds[k] ? E3b : R(0));
                 if (totm0 > R(1e-6) && Mk0r > 0)
                     E4 = PP::div(PP::div(K.one_m_bb * Hs * Mk0r, totm0) * K.F, e4den) * (h0v > K.ds[k] ? E4b : R(0));
             }
             if (!debris) {
                 VF = PP::settle(K.a13[k], K.a13sq[k], K.c109s * gz * K.ds[k]);
                 VF = VF * vfconc;
-                if (K.ds[k] > R(0.0001) && h0v < K.h0x9) VF = R(2e-3) + PP::div(fmax(h0v - K.h0x3, R(0)) * (VF - R(2e-3)), K.h0x6);
-                if (K.ds[k] > R(0.002) && h0v < K.h0x9) VF = R(2e-3) + PP::div(fmax(h0v - K.h0x3, R(0)) * (VF - R(2e-3)), K.h0x6);
+                if (K.ds[k] > R(0.0001) && h0v < K.h0x9)
+                    VF = R(2e-3) + PP::divk(fmax(h0v - K.h0x3, R(0)) * (VF - R(2e-3)), K.h0x6, (R)P.inv_h0x6, P.divk_ok);
+                if (K.ds[k] > R(0.002) && h0v < K.h0x9)
+                    VF = R(2e-3) + PP::divk(fmax(h0v - K.h0x3, R(0)) * (VF - R(2e-3)), K.h0x6, (R)P.inv_h0x6, P.divk_ok);
             }
             chtemp = u;
             const R redetach = fmin(Mk0r, dtr * (E2 + E4));
@@ -1066,7 +1091,7 @@ __device__ __forceinline__ void tile_cell(const DevParams &P, const SetV<RS> &sr
                 dep = 0;
             }
         }
-        const R dh = PP::divz(u - chtemp, K.porod);
+        const R dh = PP::divk(u - chtemp, K.porod, (R)P.invporo, P.divk_ok);
         h = h + dh;
         bulk += dh;
         totm += Mk;
@@ -1097,7 +1122,7 @@ __device__ __forceinline__ void tile_cell(const DevParams &P, const SetV<RS> &sr
         for (int k = 0; k < MAXS; k++) {
             if (k >= S) break;
             const R uk = kSlot ? (R)Uslot[k * hps] : Ureg[kSlot ? 0 : k];
-            totsed += PP::div(PP::div(uk, h), rhos);
+            totsed += PP::divk(PP::div(uk, h), rhos, (R)P.inv_rhos, P.divk_ok);
             dst.U[k * pl + q] = (RS)uk;
             if (L.stage_m) dst.M[k * pl + q] = celld[(CD_M + k) * T_I * T_J + cs];
         }

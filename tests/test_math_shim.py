@@ -90,3 +90,30 @@ def test_agreement_with_glibc(shim, glibc):
     same_sqrt = np.mean([shim.orc_m_powh(float(x)) == glibc.orc_m_powh(float(x)) for x in xs])
     assert same_pow > 0.99 and same_exp > 0.98 and same_sqrt > 0.99, (same_pow, same_exp, same_sqrt)
 
+
+
+def test_constant_divisor_by_remainder_correction_is_ieee_division():
+    """The update kernel divides by the run's constant divisors (rho_s(1-phi),
+    rho_s, J, 6 h0, 0.2, theta_s - theta_0) through their correctly rounded
+    reciprocals and two remainder corrections; it must give the IEEE
+    quotient bit for bit: millions of random dividends over the guarded
+    range, for those constants and random ones, plus the edge cases."""
+    import ctypes as C
+    import math
+    from harness import OracleRun
+    L = OracleRun.lib("shim")
+    L.orc_divk.restype = C.c_double
+    L.orc_divk.argtypes = [C.c_double, C.c_double, C.c_double]
+    L.orc_divk_check.restype = C.c_int64
+    L.orc_divk_check.argtypes = [C.c_double, C.c_int64, C.c_uint64]
+    consts = [2600 * (1 - 0.4), 2600.0, 30.0, 6 * 0.00099, 0.2, 0.4 - 0.1, 0.3]
+    rng = np.random.default_rng(7)
+    consts += [float(c) for c in np.exp2(rng.uniform(-100, 100, size=40)) * rng.uniform(1, 2, size=40)]
+    # significands right below 2 (reciprocals right above a power of two): the hardest case
+    consts += [math.ldexp(2 - 2 ** -52, e) for e in (-3, 0, 7)] + [math.ldexp(1 + 2 ** -52, e) for e in (-2, 5)]
+    for k, c in enumerate(consts):
+        assert L.orc_divk_check(c, 400000 if k < 7 else 100000, 1234 + k) == 0, c
+    for a in (0.0, -0.0, 2 ** -1074, -(2 ** -1022), 2 ** -901, 1e300, -1e308, float("inf"), float("-inf"), float("nan")):
+        for c in (1560.0, 0.2):
+            got, want = L.orc_divk(a, c, 1.0 / c), a / c
+            assert (math.isnan(got) and math.isnan(want)) or (got == want and math.copysign(1, got) == math.copysign(1, want)), (a, c)
