@@ -516,9 +516,9 @@ int swehr_ctx_create(const swehr_params *p, const swehr_inputs *in, int precisio
     Layout L0 = layout_for(p->nx, p->ny, p->sclass, p->rnum, in->ks != nullptr, has_solid, c->stagecap, 1, precision);
     make_devparams(p, in, L0, tmpP);
     if (!pooled) {
-        /* the FP64 update loads its tiles through tensor maps when the driver
+        /* the update loads its tiles through tensor maps when the driver
          * can encode them (checked again once the planes exist) */
-        c->cfg.tma = precision == SWEHR_FP64 && tma_available_f64();
+        c->cfg.tma = tma_available();
         int ce = precision == SWEHR_MIXED ? configure_step_f32(tmpP, c->num_sms, c->cfg)
                                           : configure_step_f64(tmpP, c->num_sms, c->cfg);
         if (ce) {
@@ -547,10 +547,12 @@ int swehr_ctx_create(const swehr_params *p, const swehr_inputs *in, int precisio
     CKC(cudaMemsetAsync(c->mem, 0, L.total, c->stream));
     if (precision == SWEHR_MIXED) set_views(c->B32, c->mem, L, p->sclass, in->ks != nullptr, has_solid, 1);
     else set_views(c->B64, c->mem, L, p->sclass, in->ks != nullptr, has_solid, 0);
-    if (c->cfg.tma && encode_tma_f64(c->P, c->B64, c->tm) != 0) {
+    if (c->cfg.tma && (precision == SWEHR_MIXED ? encode_tma_f32(c->P, c->B32, c->tm)
+                                                : encode_tma_f64(c->P, c->B64, c->tm)) != 0) {
         c->cfg.tma = 0;      /* the maps were refused: stage with per-thread copies instead */
         const int grid = c->cfg.grid_update;    /* the reduction partials are sized for this many blocks */
-        int ce = configure_step_f64(c->P, c->num_sms, c->cfg);
+        int ce = precision == SWEHR_MIXED ? configure_step_f32(c->P, c->num_sms, c->cfg)
+                                          : configure_step_f64(c->P, c->num_sms, c->cfg);
         c->cfg.grid_update = std::min(c->cfg.grid_update, grid);
         if (ce) {
             rc = set_err(SWEHR_CUDA_ERROR, std::string("configure: ") + cudaGetErrorString((cudaError_t)ce));

@@ -46,7 +46,7 @@ struct swehr_ctx {
     void *h_stage = nullptr;           /* the process's two pinned download buffers (set on the first large read) */
     cudaEvent_t ev_stage[2] = {};
     swehr::StepConfig cfg;
-    swehr::TmaMaps tm;      /* tensor maps of the update's tile loads (FP64, when cfg.tma) */
+    swehr::TmaMaps tm;      /* tensor maps of the update's tile loads (when cfg.tma) */
     int timing = 0;
     int64_t stagecap = 0;
     double water_init = 0;

@@ -69,6 +69,11 @@ struct BatchConfig {
     int occ_update_s[17] = {};
     int stage_m_s[17] = {};             /* stage M_k in shared memory at this class count */
     void *fn_update_s[17] = {};         /* the update kernel for that choice */
+    /* kernels built for exactly S classes (S = 7, 10; null elsewhere), used
+     * when every running scenario has S classes */
+    void *fn_update_x[17] = {};
+    size_t smem_update_x[17] = {};
+    int occ_update_x[17] = {};
 };
 
 int configure_batch_f64(int max_classes, bool budget, BatchConfig &cfg);
@@ -83,7 +88,7 @@ struct StepConfig {
     size_t smem_wave = 0, smem_update = 0;
     void *fn_update = nullptr, *fn_wave = nullptr;
     int stage_m = 1;                    /* the update stages M_k in shared memory */
-    int tma = 0;                        /* in: tensor maps exist (FP64); out: the update loads tiles through them */
+    int tma = 0;                        /* in: tensor maps can be encoded; out: the update loads tiles through them */
 };
 
 /* Pick the kernel instantiations, set their shared-memory limit and size the
@@ -99,8 +104,9 @@ int launch_step_f64(const DevParams &P, const BufsT<double> &B, Ctl *ctl, const 
 /* the update kernel's tile loads through tensor maps (FP64 form, one
  * domain): whether the driver offers the encoder, and the maps of a
  * simulation's planes (0 when all were encoded) */
-int tma_available_f64();
+int tma_available();
 int encode_tma_f64(const DevParams &P, const BufsT<double> &B, TmaMaps &tm);
+int encode_tma_f32(const DevParams &P, const BufsT<float> &B, TmaMaps &tm);
 
 /* the gz plane of the set step n reads, from its previous-step topography
  * (at creation and after the topography is written) */

@@ -6,12 +6,53 @@
 #pragma once
 #include <cuda_runtime.h>
 
+#include <cstring>
 #include <type_traits>
 
 #include "swehr_kernels.h"
 #include "swehr_tile.cuh"
 
 namespace swehr {
+
+typedef CUresult (*TensorMapEncodeFn)(CUtensorMap *, CUtensorMapDataType, cuuint32_t, void *, const cuuint64_t *,
+                                      const cuuint64_t *, const cuuint32_t *, const cuuint32_t *, CUtensorMapInterleave,
+                                      CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+/* cuTensorMapEncodeTiled through the runtime's driver entry point (no link
+ * against libcuda); null when the driver does not offer it */
+static inline TensorMapEncodeFn tensor_map_encoder()
+{
+    static TensorMapEncodeFn fn = nullptr;
+    static bool tried = false;
+    if (!tried) {
+        tried = true;
+        void *p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = (TensorMapEncodeFn)p;
+    }
+    return fn;
+}
+
+/* A 3-D tensor (ny, nx, planes) of T planes at base with the domain's pitch
+ * and plane stride, copied in boxes of box_x x box_y x 1.  The driver checks
+ * the base (16-byte aligned), the strides (multiples of 16 bytes) and the
+ * box's inner extent (a multiple of 16 bytes). */
+template <class T>
+static inline bool encode_planes(TensorMapEncodeFn enc, CUtensorMap *m, const void *base, const DevParams &P,
+                                 int planes, unsigned box_x, unsigned box_y)
+{
+    const cuuint64_t dims[3] = {(cuuint64_t)P.ny, (cuuint64_t)P.nx, (cuuint64_t)planes};
+    const cuuint64_t strides[2] = {(cuuint64_t)P.pitch * sizeof(T), (cuuint64_t)P.plane * sizeof(T)};
+    const cuuint32_t box[3] = {box_x, box_y, 1};
+    const cuuint32_t elem[3] = {1, 1, 1};
+    const CUtensorMapDataType dt = sizeof(T) == 8 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32;
+    return enc(m, dt, 3, const_cast<void *>(base), dims, strides, box, elem, CU_TENSOR_MAP_INTERLEAVE_NONE,
+               CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) ==
+           CUDA_SUCCESS;
+}
+
 inline namespace SWEHR_TILE_NS {
 
 template <class PP, class RS>
@@ -53,16 +94,49 @@ struct FormLauncher {
         return (int)cudaGetLastError();
     }
 
-    /* tile loads through tensor maps exist for the FP64 form (its planes'
-     * staged windows start on 16-byte columns) */
-    static constexpr bool kHasTma = std::is_same<RS, double>::value;
+    /* tile loads through tensor maps (both forms: every staged window starts
+     * on a 16-byte column, see Cols) */
+    static constexpr bool kHasTma = true;
 
-    template <int MAXS, bool BUDGET, bool SM, bool TMA>
-    static void *update_fn() { return (void *)k_update_tile<PP, RS, MAXS, BUDGET, SM, TMA>; }
+    /* Tensor maps for the update kernel's tile loads (planes of one domain):
+     * each state set's planes of the storage type with the halo box and the
+     * cell box, its FP64 planes with the cell box, the three topography
+     * planes with the z_prev and z window boxes, and the Ks plane.  Returns 0
+     * when every map was encoded. */
+    static int encode_tma(const DevParams &P, const BufsT<RS> &B, TmaMaps &tm)
+    {
+        TensorMapEncodeFn enc = tensor_map_encoder();
+        if (!enc) return 1;
+        memset(&tm, 0, sizeof tm);
+        const bool mixed = !std::is_same<RS, double>::value;
+        const int planes = mixed ? 9 + P.S : P_FIXED + 2 * P.S;     /* the storage-type block of a set */
+        bool ok = true;
+        for (int s = 0; s < 2; s++) {
+            ok = ok && encode_planes<RS>(enc, &tm.m[TM_HALO0 + s], B.set[s].h, P, planes, Cols<RS>::rj, HALO_ROWS);
+            ok = ok && encode_planes<RS>(enc, &tm.m[TM_CELL0 + s], B.set[s].h, P, planes, T_J, T_I);
+            if (mixed)
+                ok = ok && encode_planes<double>(enc, &tm.m[TM_CELLD0 + s], B.set[s].vinf, P, 1 + P.S, T_J, T_I);
+            else
+                ok = ok && encode_planes<double>(enc, &tm.m[TM_CELLD0 + s], B.set[s].h, P, planes, T_J, T_I);
+        }
+        ok = ok && encode_planes<double>(enc, &tm.m[TM_ZP], B.z[0], P, 3, R_J, ZP_ROWS);
+        ok = ok && encode_planes<double>(enc, &tm.m[TM_ZC], B.z[0], P, 3, R_J, ZC_ROWS);
+        if (B.ks) ok = ok && encode_planes<RS>(enc, &tm.m[TM_KS], B.ks, P, 1, T_J, T_I);
+        return ok ? 0 : 2;
+    }
+
+    template <int MAXS, bool BUDGET, bool SM, bool TMA, int NS = 0>
+    static void *update_fn() { return (void *)k_update_tile<PP, RS, MAXS, BUDGET, SM, TMA, NS>; }
 
     template <bool BUDGET, bool SM, bool TMA>
     static void *pick_u(int S)
     {
+        /* the class counts of the benchmark configurations get kernels
+         * built for exactly that many classes: their class loops have no
+         * exit tests, so the compiler interleaves the classes' independent
+         * division chains (mixed form -7 %) */
+        if (S == 7) return update_fn<8, BUDGET, SM, TMA, 7>();
+        if (S == 10) return update_fn<16, BUDGET, SM, TMA, 10>();
         if (S <= 4) return update_fn<4, BUDGET, SM, TMA>();
         if (S <= 8) return update_fn<8, BUDGET, SM, TMA>();
         return update_fn<16, BUDGET, SM, TMA>();
@@ -113,8 +187,18 @@ struct FormLauncher {
         return 0;
     }
 
-    template <int MAXS, bool BUDGET, bool SM>
-    static void *ubatch_fn() { return (void *)k_update_batch<PP, RS, MAXS, BUDGET, SM>; }
+    template <int MAXS, bool BUDGET, bool SM, int NS = 0>
+    static void *ubatch_fn() { return (void *)k_update_batch<PP, RS, MAXS, BUDGET, SM, NS>; }
+
+    /* batched kernels for exactly NS classes (every running scenario has NS) */
+    template <int MAXS, int NS>
+    static cudaError_t exact_batch(bool budget, BatchConfig &cfg)
+    {
+        void *fw = budget ? ubatch_fn<MAXS, true, true, NS>() : ubatch_fn<MAXS, false, true, NS>();
+        void *fo = budget ? ubatch_fn<MAXS, true, false, NS>() : ubatch_fn<MAXS, false, false, NS>();
+        int sm = 1;
+        return pick_staging(fw, fo, NS, cfg.smem_update_x[NS], cfg.occ_update_x[NS], sm, cfg.fn_update_x[NS]);
+    }
 
     template <bool SM>
     static void *pick_ub(int max_classes, bool budget)
@@ -141,6 +225,14 @@ struct FormLauncher {
                              cfg.fn_update_s[S]);
             if (e != cudaSuccess) return (int)e;
             if (cfg.occ_update_s[S] > cfg.occ_update) cfg.occ_update = cfg.occ_update_s[S];
+        }
+        if (max_classes >= 7) {
+            e = exact_batch<8, 7>(budget, cfg);
+            if (e != cudaSuccess) return (int)e;
+        }
+        if (max_classes >= 10) {
+            e = exact_batch<16, 10>(budget, cfg);
+            if (e != cudaSuccess) return (int)e;
         }
         /* limits for the largest shape either kernel is launched with */
         e = cudaFuncSetAttribute(fu_with, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)su);

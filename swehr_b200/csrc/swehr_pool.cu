@@ -58,6 +58,7 @@ struct swehr_pool {
     int grid_wave = 0, grid_update = 0, tuned = 0;
     int kw_sel = 0, ku_sel = 0;          /* tuned blocks per SM (0: occupancy) */
     int max_s = 1;                       /* largest class count running */
+    int min_s = 1;                       /* smallest class count running */
     size_t smem_update = 0;              /* update kernel's dynamic shared memory now */
     void *fn_update = nullptr;           /* update kernel now (staging choice for max_s) */
     cudaStream_t stream = nullptr;
@@ -205,11 +206,12 @@ static void apply_shape(swehr_pool *pl);
 /* write the running scenarios into the device table and header */
 static int rebuild_table(swehr_pool *pl)
 {
-    int k = 0, max_s = 1;
+    int k = 0, max_s = 1, min_s = 16;
     int64_t tile0 = 0, cells = 0;
     for (auto &s : pl->scen) {
         if (!s.running) continue;
         max_s = std::max(max_s, (int)s.ctx->P.S);
+        min_s = std::min(min_s, (int)s.ctx->P.S);
         s.ntiles = tiles_of(s.ctx->P, pl->cfg);     /* in the tile shape in use */
         char *slot = pl->h_tab + (size_t)k * pl->desc_bytes;
         if (pl->precision == SWEHR_MIXED)
@@ -261,6 +263,7 @@ static int rebuild_table(swehr_pool *pl)
     pl->total_tiles = tile0;
     pl->running_cells = cells;
     pl->max_s = max_s;
+    pl->min_s = std::min(min_s, max_s);
     pl->dirty = false;
     apply_shape(pl);
     return SWEHR_OK;
@@ -310,11 +313,25 @@ static void set_grids(swehr_pool *pl, int kw, int ku)
  * kernel's staging is sized by the largest class count present, so a pool
  * that admits up to 16 classes still runs 7-class batches at the 7-class
  * occupancy */
+/* the running scenarios all have the class count of a kernel built for
+ * exactly that many classes */
+static bool exact_classes(const swehr_pool *pl, const BatchConfig &c)
+{
+    return pl->min_s == pl->max_s && c.fn_update_x[pl->max_s] != nullptr;
+}
+
+static int update_occupancy(const swehr_pool *pl, const BatchConfig &c)
+{
+    return exact_classes(pl, c) ? c.occ_update_x[pl->max_s] : c.occ_update_s[pl->max_s];
+}
+
 static void apply_shape(swehr_pool *pl)
 {
-    pl->smem_update = pl->cfg.smem_update_s[pl->max_s];
-    pl->fn_update = pl->cfg.fn_update_s[pl->max_s];
-    const int occ_u = pl->cfg.occ_update_s[pl->max_s];
+    const int S = pl->max_s;
+    const bool exact = exact_classes(pl, pl->cfg);
+    pl->smem_update = exact ? pl->cfg.smem_update_x[S] : pl->cfg.smem_update_s[S];
+    pl->fn_update = exact ? pl->cfg.fn_update_x[S] : pl->cfg.fn_update_s[S];
+    const int occ_u = update_occupancy(pl, pl->cfg);
     const int ku = pl->ku_sel ? std::min(pl->ku_sel, occ_u) : occ_u;
     const int kw = pl->kw_sel ? pl->kw_sel : pl->cfg.occ_wave;
     set_grids(pl, kw, ku);
@@ -570,7 +587,7 @@ int swehr_pool_tune(swehr_pool *pl, int64_t steps_per_trial, swehr_pool_stats *s
     int trials[2], occ_u[2];
     std::vector<std::pair<int, int>> cand;
     for (int sh = 0; sh < nsh; sh++) {
-        occ_u[sh] = pl->shapes[sh].occ_update_s[pl->max_s];
+        occ_u[sh] = update_occupancy(pl, pl->shapes[sh]);
         trials[sh] = std::max(pl->shapes[sh].occ_wave, occ_u[sh]);
         for (int k = 1; k <= trials[sh]; k++) cand.push_back({sh, k});
     }

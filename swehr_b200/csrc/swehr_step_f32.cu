@@ -26,6 +26,11 @@ int launch_step_f32(const DevParams &P, const BufsT<float> &B, Ctl *ctl, const d
     return FormLauncher<PolicyF32, float>::launch(P, B, ctl, rain, partials, stage, saveflow, tm, cfg, s, ev0, ev1);
 }
 
+int encode_tma_f32(const DevParams &P, const BufsT<float> &B, TmaMaps &tm)
+{
+    return FormLauncher<PolicyF32, float>::encode_tma(P, B, tm);
+}
+
 int configure_batch_f32(int max_classes, bool budget, BatchConfig &cfg)
 {
     return FormLauncher<PolicyF32, float>::configure_batch(max_classes, budget, cfg);

@@ -274,17 +274,24 @@ __device__ __forceinline__ TileCoord tile_coord(const DevParams &P, int64_t tile
 
 /* -------------------------------------------------------------- staging ---
  * Every global load of a tile is issued up front as an asynchronous copy
- * (cp.async, 2 elements per copy) into shared memory, so the arithmetic never
- * waits on HBM and other CTAs on the SM compute while this one's copies fly.
- *   halo planes  h hu hv totsed dep U_1..U_S   10 rows x 36 columns
+ * (cp.async of 16 bytes, or one tensor-map box per plane) into shared memory,
+ * so the arithmetic never waits on HBM and other CTAs on the SM compute while
+ * this one's copies fly.
+ *   halo planes  h hu hv totsed dep U_1..U_S   10 rows x (32 + 2 pad) columns
  *   cell planes  totm maxvel maxdep [ks] (RS), vinf M_1..M_S (double)   8 x 32
- *   topography   z_prev 12 x 36, z 10 x 36
- * Row r of a halo plane is grid row i0-1+r; column c is grid column
- * (0-based) j0-3+c, so halo cell (hi, hj) sits at (hi, hj+1) and the first
- * column is 16-byte aligned.  (Counts above are for the 8 x 32 tile.)  Rows or columns outside the grid are not
- * loaded: ghosts are resolved from their source cells afterwards
- * (SWEHR.c:816-1035). */
-#define R_J (T_J + 4)       /* staged columns */
+ *   topography   z_prev 12 x 36, z 10 x 36 (double)
+ * A staged row of a plane of T starts pad = 16 / sizeof(T) columns left of
+ * the tile: row r is grid row i0-1+r, column c is grid column (0-based)
+ * j0-1-pad+c, so every staged row starts 16-byte aligned in HBM and halo
+ * cell (hi, hj) sits at (hi, hj+pad-1).  (Counts above are for the 8 x 32
+ * tile.)  Rows or columns outside the grid are not loaded: ghosts are
+ * resolved from their source cells afterwards (SWEHR.c:816-1035). */
+template <class T>
+struct Cols {
+    static constexpr int pad = 16 / (int)sizeof(T);   /* staged columns left of the tile */
+    static constexpr int rj = T_J + 2 * pad;          /* staged columns per row */
+};
+#define R_J (T_J + 4)       /* staged columns of the (double) topography windows */
 #define HALO_ROWS H_I
 #define ZP_ROWS (T_I + 4)
 #define ZC_ROWS (T_I + 2)
@@ -296,7 +303,7 @@ struct StagedLayout {
     /* byte offsets from the start of dynamic shared memory */
     size_t halo, cell_r, cell_d, zp, zc, u, v, g, c, sed, fx, fy, up, red, total;
     int nhalo, ncellr, ncelld;
-    int hps;              /* elements from one halo plane to the next (rows x R_J, rounded to 128 bytes) */
+    int hps;              /* elements from one halo plane to the next (rows x staged columns, rounded to 128 bytes) */
     int stage_m;          /* M_k staged here (else read from global memory by the cell stage) */
     /* stage_m: staging M_k costs 2 KB of shared memory per class; the
      * launcher picks the kernel that stages it only where that costs no
@@ -307,7 +314,8 @@ struct StagedLayout {
         size_t o = 0;
         /* every region starts 128-byte aligned (a tile copy's destination) */
         auto take = [&](size_t bytes) { size_t at = o; o += (bytes + 127) / 128 * 128; return at; };
-        L.hps = (int)(((size_t)HALO_ROWS * R_J * rs + 127) / 128 * 128 / rs);
+        const size_t rj = (size_t)T_J + 2 * (16 / rs);
+        L.hps = (int)(((size_t)HALO_ROWS * rj * rs + 127) / 128 * 128 / rs);
         L.stage_m = stage_m;
         L.nhalo = 5 + S;
         L.ncellr = 4;
@@ -359,48 +367,58 @@ __device__ __forceinline__ void cp_pair(void *dst, const T *src)
     __pipeline_memcpy_async(dst, src, 2 * sizeof(T));
 }
 
+/* 16-byte copy global -> shared (both addresses 16-byte aligned) */
+__device__ __forceinline__ void cp16(void *dst, const void *src) { __pipeline_memcpy_async(dst, src, 16); }
+
 /* Issue the tile's asynchronous copies (halo planes, z_prev and z windows,
- * cell planes).  Each thread owns fixed (row, pair) slots and walks the
- * planes with a pointer step, so the per-copy cost is one add. */
-template <class RS>
+ * cell planes).  Each thread owns fixed (row, vector) slots and walks the
+ * planes with a pointer step, so the per-copy cost is one add.  Halo rows
+ * and topography windows move 16 bytes per copy (2 doubles or 4 floats). */
+template <class RS, int NS = 0>
 __device__ __forceinline__ void stage_load(const DevParams &P, const SetV<RS> &src, const double *__restrict__ zp,
                                            const double *__restrict__ zc, const RS *__restrict__ ks, TileCoord tc,
                                            unsigned char *smb, const StagedLayout &L)
 {
     const int64_t pl = P.plane;
-    const int c0 = tc.j0 - 3;                                  /* 0-based grid column of staged column 0 */
+    const int S = NS ? NS : P.S;
+    constexpr int VEC = Cols<RS>::pad;                         /* elements per 16-byte copy */
+    constexpr int RJ = Cols<RS>::rj, NV = RJ / VEC;            /* copies per halo row: 18 (double), 10 (float) */
+    const int c0 = tc.j0 - 1 - Cols<RS>::pad;                  /* 0-based grid column of staged column 0 */
     const int tid = threadIdx.x;
-    /* halo planes: 10 rows x 18 pairs = 180 slots */
-    if (tid < HALO_ROWS * (R_J / 2)) {
-        const int r = tid / (R_J / 2), k2 = tid - r * (R_J / 2);
-        const int gi = tc.i0 - 1 + r, col = c0 + 2 * k2;
+    static_assert(HALO_ROWS * NV <= TILE_THREADS, "one halo slot per thread");
+    /* halo planes: 10 rows x NV vectors */
+    if (tid < HALO_ROWS * NV) {
+        const int r = tid / NV, kv = tid - r * NV;
+        const int gi = tc.i0 - 1 + r, col = c0 + VEC * kv;
         /* columns past ny are row padding no cell reads (a ghost column
-         * takes its source cell's values): not loaded */
+         * takes its source cell's values): not loaded; a vector starting
+         * before ny ends inside the row (pitch is a multiple of 32) */
         if (gi >= 1 && gi <= P.nx && col >= 0 && col < P.ny) {
             const int64_t go = (int64_t)(gi - 1) * P.pitch + col;
-            RS *d = reinterpret_cast<RS *>(smb + L.halo) + r * R_J + 2 * k2;
+            RS *d = reinterpret_cast<RS *>(smb + L.halo) + r * RJ + VEC * kv;
             const int ps = L.hps;
-            cp_pair(d + HP_H * ps, src.h + go);
-            cp_pair(d + HP_HU * ps, src.hu + go);
-            cp_pair(d + HP_HV * ps, src.hv + go);
-            cp_pair(d + HP_TS * ps, src.totsed + go);
-            cp_pair(d + HP_DEP * ps, src.dep + go);
+            cp16(d + HP_H * ps, src.h + go);
+            cp16(d + HP_HU * ps, src.hu + go);
+            cp16(d + HP_HV * ps, src.hv + go);
+            cp16(d + HP_TS * ps, src.totsed + go);
+            cp16(d + HP_DEP * ps, src.dep + go);
             const RS *u = src.U + go;
-            for (int k = 0; k < P.S; k++) cp_pair(d + (HP_U + k) * ps, u + (int64_t)k * pl);
+            for (int k = 0; k < S; k++) cp16(d + (HP_U + k) * ps, u + (int64_t)k * pl);
         }
     }
     /* topography: z_prev 12 rows, z 10 rows, 18 pairs each */
     {
-        const int slot = tid < HALO_ROWS * (R_J / 2) ? tid + (256 - HALO_ROWS * (R_J / 2)) : tid - HALO_ROWS * (R_J / 2);
+        constexpr int NHS = HALO_ROWS * NV;
+        const int slot = tid < NHS ? tid + (TILE_THREADS - NHS) : tid - NHS;
         const int nzs = (ZP_ROWS + ZC_ROWS) * (R_J / 2);                   /* 396 */
         for (int s = slot; s < nzs; s += TILE_THREADS) {
             const bool isp = s < ZP_ROWS * (R_J / 2);
             const int s2 = isp ? s : s - ZP_ROWS * (R_J / 2);
             const int r = s2 / (R_J / 2), k2 = s2 - r * (R_J / 2);
-            const int gi = (isp ? tc.i0 - 2 : tc.i0 - 1) + r, col = c0 + 2 * k2;
+            const int gi = (isp ? tc.i0 - 2 : tc.i0 - 1) + r, col = tc.j0 - 3 + 2 * k2;   /* double windows: pad 2 */
             if (gi < 1 || gi > P.nx || col < 0 || col >= P.ny) continue;
             double *d = reinterpret_cast<double *>(smb + (isp ? L.zp : L.zc)) + r * R_J + 2 * k2;
-            cp_pair(d, (isp ? zp : zc) + (int64_t)(gi - 1) * P.pitch + col);
+            cp16(d, (isp ? zp : zc) + (int64_t)(gi - 1) * P.pitch + col);
         }
     }
     /* cell planes: 8 rows x 16 pairs = 128 slots; threads 128..255 */
@@ -420,48 +438,70 @@ __device__ __forceinline__ void stage_load(const DevParams &P, const SetV<RS> &s
             cp_pair(cd + CD_VINF * ps, src.vinf + go);
             if (L.stage_m) {
                 const double *m = src.M + go;
-                for (int k = 0; k < P.S; k++) cp_pair(cd + (CD_M + k) * ps, m + (int64_t)k * pl);
+                for (int k = 0; k < S; k++) cp_pair(cd + (CD_M + k) * ps, m + (int64_t)k * pl);
             }
         }
     }
     __pipeline_commit();
 }
 
-/* The same staging as stage_load as tensor-map box copies (FP64 planes of
- * one domain), issued by one thread onto the tile's mbarrier: halo boxes
- * R_J x halo rows at column j0-3, row i0-2 (0-based), the z_prev window one
- * row higher and taller, cell boxes T_J x T_I at (j0-1, i0-1).  x = j0-3 is
- * even, so every box starts on a 16-byte column boundary; rows or columns
- * outside the grid arrive as zeros. */
+/* Plane numbers of a state set in its tensor maps: the plain form's set
+ * is one FP64 block (swehr_device.cuh), the mixed form's an FP32 block
+ * (h hu hv maxvel maxdep totm dep totsed gz U_1..U_S) followed by an FP64
+ * block (vinf M_1..M_S).  `d_*` index the set's FP64 planes. */
+template <class RS>
+struct SetPlanes;
+template <>
+struct SetPlanes<double> {
+    enum { h = P_H, hu = P_HU, hv = P_HV, maxvel = P_MAXVEL, maxdep = P_MAXDEP, totm = P_TOTM, dep = P_DEP,
+           totsed = P_TOTSED, U = P_FIXED, d_vinf = P_VINF };
+    static __device__ __forceinline__ int d_M(int S) { return P_FIXED + S; }
+};
+template <>
+struct SetPlanes<float> {
+    enum { h = 0, hu = 1, hv = 2, maxvel = 3, maxdep = 4, totm = 5, dep = 6, totsed = 7, U = 9, d_vinf = 0 };
+    static __device__ __forceinline__ int d_M(int) { return 1; }
+};
+
+/* The same staging as stage_load as tensor-map box copies (planes of one
+ * domain), issued by one thread onto the tile's mbarrier: halo boxes of
+ * Cols<RS>::rj columns x halo rows at column j0-1-pad, row i0-2 (0-based),
+ * the z_prev window one row higher and taller (doubles, column j0-3), cell
+ * boxes T_J x T_I at (j0-1, i0-1).  j0-1 is a multiple of T_J and pad is 16
+ * bytes of the plane's type, so every box starts on a 16-byte column
+ * boundary; rows or columns outside the grid arrive as zeros. */
+template <class RS>
 __device__ __forceinline__ void stage_load_tma(const DevParams &P, const TmaMaps &tm, int set, int64_t n,
                                                TileCoord tc, unsigned char *smb, const StagedLayout &L,
                                                uint64_t *bar)
 {
-    const uint32_t hb = (uint32_t)(HALO_ROWS * R_J * sizeof(double));
-    const uint32_t cb = (uint32_t)(T_I * T_J * sizeof(double));
+    typedef SetPlanes<RS> SP;
+    const uint32_t hb = (uint32_t)(HALO_ROWS * Cols<RS>::rj * sizeof(RS));
+    const uint32_t cbr = (uint32_t)(T_I * T_J * sizeof(RS)), cbd = (uint32_t)(T_I * T_J * sizeof(double));
     const uint32_t bytes = (uint32_t)(5 + P.S) * hb + (uint32_t)((ZP_ROWS + ZC_ROWS) * R_J * sizeof(double)) +
-                           (3u + (P.has_ks ? 1u : 0u) + 1u + (L.stage_m ? (uint32_t)P.S : 0u)) * cb;
+                           (3u + (P.has_ks ? 1u : 0u)) * cbr + (1u + (L.stage_m ? (uint32_t)P.S : 0u)) * cbd;
     mbar_expect_tx(bar, bytes);
-    const CUtensorMap *mh = &tm.m[TM_HALO0 + set], *mc = &tm.m[TM_CELL0 + set];
-    const int hx = tc.j0 - 3, hy = tc.i0 - 2, cx = tc.j0 - 1, cy = tc.i0 - 1;
-    double *halo = reinterpret_cast<double *>(smb + L.halo);
-    tma_load_3d(halo + HP_H * L.hps, mh, bar, hx, hy, P_H);
-    tma_load_3d(halo + HP_HU * L.hps, mh, bar, hx, hy, P_HU);
-    tma_load_3d(halo + HP_HV * L.hps, mh, bar, hx, hy, P_HV);
-    tma_load_3d(halo + HP_TS * L.hps, mh, bar, hx, hy, P_TOTSED);
-    tma_load_3d(halo + HP_DEP * L.hps, mh, bar, hx, hy, P_DEP);
-    for (int k = 0; k < P.S; k++) tma_load_3d(halo + (HP_U + k) * L.hps, mh, bar, hx, hy, P_FIXED + k);
-    tma_load_3d(smb + L.zp, &tm.m[TM_ZP], bar, hx, tc.i0 - 3, (int)((n + 2) % 3));
-    tma_load_3d(smb + L.zc, &tm.m[TM_ZC], bar, hx, hy, (int)(n % 3));
-    double *cr = reinterpret_cast<double *>(smb + L.cell_r), *cd = reinterpret_cast<double *>(smb + L.cell_d);
+    const CUtensorMap *mh = &tm.m[TM_HALO0 + set], *mc = &tm.m[TM_CELL0 + set], *md = &tm.m[TM_CELLD0 + set];
+    const int hx = tc.j0 - 1 - Cols<RS>::pad, hy = tc.i0 - 2, zx = tc.j0 - 3, cx = tc.j0 - 1, cy = tc.i0 - 1;
+    RS *halo = reinterpret_cast<RS *>(smb + L.halo);
+    tma_load_3d(halo + HP_H * L.hps, mh, bar, hx, hy, SP::h);
+    tma_load_3d(halo + HP_HU * L.hps, mh, bar, hx, hy, SP::hu);
+    tma_load_3d(halo + HP_HV * L.hps, mh, bar, hx, hy, SP::hv);
+    tma_load_3d(halo + HP_TS * L.hps, mh, bar, hx, hy, SP::totsed);
+    tma_load_3d(halo + HP_DEP * L.hps, mh, bar, hx, hy, SP::dep);
+    for (int k = 0; k < P.S; k++) tma_load_3d(halo + (HP_U + k) * L.hps, mh, bar, hx, hy, SP::U + k);
+    tma_load_3d(smb + L.zp, &tm.m[TM_ZP], bar, zx, tc.i0 - 3, (int)((n + 2) % 3));
+    tma_load_3d(smb + L.zc, &tm.m[TM_ZC], bar, zx, hy, (int)(n % 3));
+    RS *cr = reinterpret_cast<RS *>(smb + L.cell_r);
+    double *cd = reinterpret_cast<double *>(smb + L.cell_d);
     const int ps = T_I * T_J;
-    tma_load_3d(cr + CR_TOTM * ps, mc, bar, cx, cy, P_TOTM);
-    tma_load_3d(cr + CR_MAXVEL * ps, mc, bar, cx, cy, P_MAXVEL);
-    tma_load_3d(cr + CR_MAXDEP * ps, mc, bar, cx, cy, P_MAXDEP);
+    tma_load_3d(cr + CR_TOTM * ps, mc, bar, cx, cy, SP::totm);
+    tma_load_3d(cr + CR_MAXVEL * ps, mc, bar, cx, cy, SP::maxvel);
+    tma_load_3d(cr + CR_MAXDEP * ps, mc, bar, cx, cy, SP::maxdep);
     if (P.has_ks) tma_load_3d(cr + CR_KS * ps, &tm.m[TM_KS], bar, cx, cy, 0);
-    tma_load_3d(cd + CD_VINF * ps, mc, bar, cx, cy, P_VINF);
+    tma_load_3d(cd + CD_VINF * ps, md, bar, cx, cy, SP::d_vinf);
     if (L.stage_m)
-        for (int k = 0; k < P.S; k++) tma_load_3d(cd + (CD_M + k) * ps, mc, bar, cx, cy, P_FIXED + P.S + k);
+        for (int k = 0; k < P.S; k++) tma_load_3d(cd + (CD_M + k) * ps, md, bar, cx, cy, SP::d_M(P.S) + k);
 }
 
 /* slopes from a staged topography tile, same operations as slope_x/slope_y
@@ -483,12 +523,13 @@ __device__ __forceinline__ double sslope_y(const DevParams &P, const double *zs,
 /* Derived halo values from the staged planes: h, u = hu/h, v = hv/h (0 when
  * dry), GZ of the previous step and sqrt(GZ h) for left/lower face cells,
  * SED_k.  Ghost cells read their source cell (SWEHR.c:816-1035). */
-template <class PP, class RS>
+template <class PP, class RS, int NS = 0>
 __device__ __forceinline__ void stage_derive(const DevParams &P, const SetV<RS> &src, TileCoord tc, unsigned char *smb,
                                              const StagedLayout &L, typename PP::R inh, typename PP::R inhv,
                                              typename PP::R insed)
 {
     typedef typename PP::R R;
+    const int S = NS ? NS : P.S;
     const RealC<R> &K = kc<R>(P);
     const RS *halo = reinterpret_cast<const RS *>(smb + L.halo);
     const double *zps = reinterpret_cast<const double *>(smb + L.zp);
@@ -503,8 +544,9 @@ __device__ __forceinline__ void stage_derive(const DevParams &P, const SetV<RS> 
         if (hcorner || gi > P.nx + 1 || gj > P.ny + 1 || (gx && gy)) continue;
         const int si = gi < 1 ? 1 : (gi > P.nx ? P.nx : gi);
         const int sj = gj < 1 ? 1 : (gj > P.ny ? P.ny : gj);
-        const int sr = si - (tc.i0 - 1), scol = sj - (tc.j0 - 2);          /* staged position of the source */
-        const int so = sr * R_J + scol;
+        /* staged position of the source in the RS planes, and its column in the topography windows */
+        const int sr = si - (tc.i0 - 1), scol = sj - tc.j0 + Cols<RS>::pad, zcol = sj - tc.j0 + 2;
+        const int so = sr * Cols<RS>::rj + scol;
         const bool inflow = gj == P.ny + 1 && P.inflow;
         R h, hu, hv;
         if (inflow) {
@@ -520,7 +562,7 @@ __device__ __forceinline__ void stage_derive(const DevParams &P, const SetV<RS> 
         if (h > K.hfilm) { u = PP::div(hu, h); v = PP::div(hv, h); }
         if (gx || gy) {
             /* ghost cells are never read through the staged planes: keep h there */
-            reinterpret_cast<RS *>(smb + L.halo)[HP_H * L.hps + hi * R_J + hj + 1] = (RS)h;
+            reinterpret_cast<RS *>(smb + L.halo)[HP_H * L.hps + hi * Cols<RS>::rj + hj + Cols<RS>::pad - 1] = (RS)h;
         }
         su[idx] = u;
         sv[idx] = v;
@@ -533,7 +575,7 @@ __device__ __forceinline__ void stage_derive(const DevParams &P, const SetV<RS> 
             } else {
                 /* GZ of the previous step at the source cell, SWEHR.c:1279 via z_prev */
                 const int zr = si - (tc.i0 - 2);
-                const R sx = (R)sslope_x(P, zps, zr, scol, si), sy = (R)sslope_y(P, zps, zr, scol, sj);
+                const R sx = (R)sslope_x(P, zps, zr, zcol, si), sy = (R)sslope_y(P, zps, zr, zcol, sj);
                 g = PP::div(K.g, PP::sqrtp(sx * sx + sy * sy + 1));
             }
             sg[idx] = g;
@@ -550,9 +592,10 @@ __device__ __forceinline__ void stage_derive(const DevParams &P, const SetV<RS> 
         };
         if (PP::kRollClasses) {          /* one division sequence in the code, not four */
 #pragma unroll 1
-            for (int k = 0; k < P.S; k++) sed_k(k);
+            for (int k = 0; k < S; k++) sed_k(k);
         } else {
-            for (int k = 0; k < P.S; k++) sed_k(k);
+#pragma unroll
+            for (int k = 0; k < S; k++) sed_k(k);
         }
     }
 }
@@ -864,7 +907,7 @@ __device__ __forceinline__ void solid_cell(const DevParams &P, const SetV<RS> &s
     zn[q] = zc[q];
 }
 
-template <class PP, class RS, int MAXS, bool BUDGET>
+template <class PP, class RS, int MAXS, bool BUDGET, int NS = 0>
 __device__ __forceinline__ void tile_cell(const DevParams &P, const SetV<RS> &src, const SetV<RS> &dst,
                                           const double *__restrict__ zp, const double *__restrict__ zc,
                                           double *__restrict__ zn, const unsigned char *smb, const StagedLayout &L,
@@ -882,10 +925,11 @@ __device__ __forceinline__ void tile_cell(const DevParams &P, const SetV<RS> &sr
         solid_cell<PP, RS, MAXS, BUDGET>(P, src, dst, zc, zn, q, acc);
         return;
     }
-    const int S = P.S;
+    const int S = NS ? NS : P.S;
     const R hfilm = K.hfilm, rhos = K.rhos, rhow = K.rhow, one = 1, half = R(0.5);
     const int hs = (ti + 1) * H_J + (tj + 1);                      /* this cell in halo coords */
-    const int so = (ti + 1) * R_J + (tj + 2);                      /* ... and in the staged planes */
+    constexpr int RJ = Cols<RS>::rj;
+    const int so = (ti + 1) * RJ + (tj + Cols<RS>::pad);          /* ... and in the staged planes */
     const int cs = ti * T_J + tj;                                  /* ... and in the cell planes */
     const RS *halo = reinterpret_cast<const RS *>(smb + L.halo);
     const RS *cellr = reinterpret_cast<const RS *>(smb + L.cell_r);
@@ -929,7 +973,7 @@ __device__ __forceinline__ void tile_cell(const DevParams &P, const SetV<RS> &sr
     R gammax = 0, gammay = 0;
     if (i > 1 && i < P.nx)
         gammax -= PP::div((rhos - rho0c) * gz * h0v * h0v, 2 * rho0c) * half * K.oneoverdx
-                  * ((R)sTS[so + R_J] - (R)sTS[so - R_J]);
+                  * ((R)sTS[so + RJ] - (R)sTS[so - RJ]);
     if (j > 1 && j < P.ny)
         gammay -= PP::div((rhos - rho0c) * gz * h0v * h0v, 2 * rho0c) * half * K.oneoverdx
                   * ((R)sTS[so + 1] - (R)sTS[so - 1]);
@@ -939,7 +983,7 @@ __device__ __forceinline__ void tile_cell(const DevParams &P, const SetV<RS> &sr
         const R rho0 = K.rho0;
         const R A = rho0 * gz * dep0 + rho0c * gz * h0v;
         const R s = fabs(sy);
-        const R depx = fabs((R)sDEP[i < P.nx ? so + R_J : so]) + fabs((R)sDEP[i > 1 ? so - R_J : so]);
+        const R depx = fabs((R)sDEP[i < P.nx ? so + RJ : so]) + fabs((R)sDEP[i > 1 ? so - RJ : so]);
         const R depy = fabs((R)sDEP[j < P.ny ? so + 1 : so]) + fabs((R)sDEP[j > 1 ? so - 1 : so]);
         const R pb = fabs(dep0) * rho0 * fabs(gz) * half * K.oneoverdx * fmax(depx, depy);
         const R w = rhow * gz * (dep0 + h0v);
@@ -1254,7 +1298,7 @@ __device__ __forceinline__ void stage_sample_tile(const DevParams &P, const SetV
 
 /* Update of one tile: stages A (staging), B (faces), C (cells).  The whole
  * block calls it. */
-template <class PP, class RS, int MAXS, bool BUDGET, bool TMA = false>
+template <class PP, class RS, int MAXS, bool BUDGET, bool TMA = false, int NS = 0>
 __device__ __forceinline__ void update_tile(const DevParams &P, const BufsT<RS> &B, int64_t n, double t, double dt,
                                             double Rr, TileCoord tc, unsigned char *smb, const StagedLayout &L,
                                             Acc2<MAXS, BUDGET> &acc, const TmaMaps *tm = nullptr,
@@ -1277,17 +1321,17 @@ __device__ __forceinline__ void update_tile(const DevParams &P, const BufsT<RS> 
          * (the barrier ending it); order them before the copies that land */
         if (threadIdx.x == 0) {
             fence_proxy_async_smem();
-            stage_load_tma(P, *tm, (int)(n & 1), n, tc, smb, L, bar);
+            stage_load_tma<RS>(P, *tm, (int)(n & 1), n, tc, smb, L, bar);
         }
         if (!mbar_wait_bounded(bar, *phase & 1u) && threadIdx.x == 0) ctl->dev_error = 1;
         *phase += 1;
         __syncthreads();
     } else {
-        stage_load<RS>(P, src, zp, zc, B.ks, tc, smb, L);
+        stage_load<RS, NS>(P, src, zp, zc, B.ks, tc, smb, L);
         __pipeline_wait_prior(0);
         __syncthreads();
     }
-    stage_derive<PP, RS>(P, src, tc, smb, L, (R)inh, (R)inhv, (R)insed);
+    stage_derive<PP, RS, NS>(P, src, tc, smb, L, (R)inh, (R)inhv, (R)insed);
     __syncthreads();
     const RS *sh = staged_h<RS>(smb, L);
     /* stage B: every face of the tile (SWEHR.c:1099-1230) */
@@ -1298,7 +1342,7 @@ __device__ __forceinline__ void update_tile(const DevParams &P, const BufsT<RS> 
             const int gi = tc.i0 - 1 + fi, gj = tc.j0 + fj;
             if (gj > P.ny || gi > P.nx) continue;
             const int Lh = fi * H_J + fj + 1, Rh = Lh + H_J;
-            const R hl = (R)sh[fi * R_J + fj + 2], hr = (R)sh[(fi + 1) * R_J + fj + 2];
+            const R hl = (R)sh[fi * Cols<RS>::rj + fj + Cols<RS>::pad], hr = (R)sh[(fi + 1) * Cols<RS>::rj + fj + Cols<RS>::pad];
             int var = 0;                 /* 1: solid left, 2: solid right (SWEHR.c:1137-1146) */
             if (P.has_solid && gi >= 1 && gi < P.nx) {
                 const bool sl = solid_at(P, B.solid, gi, gj), sr = solid_at(P, B.solid, gi + 1, gj);
@@ -1323,7 +1367,8 @@ __device__ __forceinline__ void update_tile(const DevParams &P, const BufsT<RS> 
             const int gi = tc.i0 + fi, gj = tc.j0 - 1 + fj;
             if (gi > P.nx || gj > P.ny) continue;
             const int Lh = (fi + 1) * H_J + fj, Rh = Lh + 1;
-            const R hl = (R)sh[(fi + 1) * R_J + fj + 1], hr = (R)sh[(fi + 1) * R_J + fj + 2];
+            const R hl = (R)sh[(fi + 1) * Cols<RS>::rj + fj + Cols<RS>::pad - 1],
+                    hr = (R)sh[(fi + 1) * Cols<RS>::rj + fj + Cols<RS>::pad];
             int var = 0;                 /* 1: solid below, 2: solid above (SWEHR.c:1205-1214) */
             if (P.has_solid && gj >= 1) {
                 const bool sl = solid_at(P, B.solid, gi, gj), sr = solid_at(P, B.solid, gi, gj + 1);
@@ -1343,7 +1388,7 @@ __device__ __forceinline__ void update_tile(const DevParams &P, const BufsT<RS> 
         }
     }
     __syncthreads();
-    tile_cell<PP, RS, MAXS, BUDGET>(P, src, dst, zp, zc, zn, smb, L, tc, t, dt, Rr, acc, B.solid, B.z0);
+    tile_cell<PP, RS, MAXS, BUDGET, NS>(P, src, dst, zp, zc, zn, smb, L, tc, t, dt, Rr, acc, B.solid, B.z0);
     __syncthreads();
 }
 
@@ -1425,7 +1470,7 @@ __device__ __forceinline__ void budget_fold(Ctl *ctl, int m, double hi, double l
     ctl->budget_lo[m] = Ll;
 }
 
-template <class PP, class RS, int MAXS, bool BUDGET, bool STAGE_M, bool TMA>
+template <class PP, class RS, int MAXS, bool BUDGET, bool STAGE_M, bool TMA, int NS>
 __global__ void __launch_bounds__(TILE_THREADS, PP::kMinBlocks) k_update_tile(const DevParams P, const BufsT<RS> B, Ctl *ctl,
                                                                   const double *__restrict__ rain, double *partials,
                                                                   double *stage, double *saveflow,
@@ -1457,7 +1502,7 @@ __global__ void __launch_bounds__(TILE_THREADS, PP::kMinBlocks) k_update_tile(co
     acc_zero(acc);
     const int64_t ntiles = (int64_t)((P.nx + T_I - 1) / T_I) * ((P.ny + T_J - 1) / T_J);
     for (int64_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x)
-        update_tile<PP, RS, MAXS, BUDGET, TMA>(P, B, n, t, dt, Rr, tile_coord(P, tile), smb, L, acc, &tm, &tma_bar,
+        update_tile<PP, RS, MAXS, BUDGET, TMA, NS>(P, B, n, t, dt, Rr, tile_coord(P, tile), smb, L, acc, &tm, &tma_bar,
                                                &tma_phase, ctl);
     double *red = reinterpret_cast<double *>(smb + L.red);
     if (BUDGET) budget_block_sum(acc, red);
@@ -1623,7 +1668,7 @@ __global__ void __launch_bounds__(TILE_THREADS) k_wave_batch(const BatchHdr<RS> 
 
 /* Batched update pass, with the same per-scenario runs: budget accumulators
  * carry across a run and are summed, counted and folded once per run. */
-template <class PP, class RS, int MAXS, bool BUDGET, bool STAGE_M>
+template <class PP, class RS, int MAXS, bool BUDGET, bool STAGE_M, int NS>
 __global__ void __launch_bounds__(TILE_THREADS, PP::kMinBlocks) k_update_batch(const BatchHdr<RS> *__restrict__ hdr)
 {
     typedef typename PP::R R;
@@ -1691,7 +1736,7 @@ __global__ void __launch_bounds__(TILE_THREADS, PP::kMinBlocks) k_update_batch(c
                 __syncthreads();
             }
             if (!snap.go) continue;
-            update_tile<PP, RS, MAXS, BUDGET>(sd.P, sd.B, snap.n, snap.t, snap.dt, snap.rain,
+            update_tile<PP, RS, MAXS, BUDGET, false, NS>(sd.P, sd.B, snap.n, snap.t, snap.dt, snap.rain,
                                               tile_coord(sd.P, g - sd.tile0), smb, L, acc);
             run++;
         }

@@ -21,16 +21,20 @@
 
 namespace swehr {
 
-/* tensor maps of one simulation (FP64 planes), passed to the update kernel
- * as a __grid_constant__ parameter */
+/* tensor maps of one simulation, passed to the update kernel as a
+ * __grid_constant__ parameter.  The halo and cell maps cover the set's
+ * planes of its storage type (every plane in the plain form, the FP32 block
+ * in the mixed form), the CELLD maps its FP64 planes. */
 enum {
-    TM_HALO0 = 0,    /* state set 0, every plane; box R_J x halo rows x 1 */
+    TM_HALO0 = 0,    /* state set 0, every plane; box staged columns x halo rows x 1 */
     TM_HALO1,        /* state set 1 */
     TM_CELL0,        /* state set 0, every plane; box tile columns x tile rows x 1 */
     TM_CELL1,        /* state set 1 */
     TM_ZP,           /* the three topography planes; box R_J x (tile rows + 4) x 1 */
     TM_ZC,           /* the three topography planes; box R_J x (tile rows + 2) x 1 */
     TM_KS,           /* the Ks plane; box tile columns x tile rows x 1 */
+    TM_CELLD0,       /* state set 0, its FP64 planes (vinf, M_k); box tile columns x tile rows x 1 */
+    TM_CELLD1,       /* state set 1 */
     TM_COUNT
 };
 
