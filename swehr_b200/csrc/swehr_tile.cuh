@@ -117,6 +117,29 @@ struct PolicyF64 {
         if (a == 0 && c > 0) return a;
         return a / c;
     }
+    /* The flow-detachment terms E3 = (num / J) m and E4 = ((A / T) F / e) m
+     * of SWEHR.c:1365-1375, where the factor m (the excess stream power) is
+     * an exact zero wherever flow is below its critical power: the IEEE
+     * product of a finite quotient with a zero is a zero whose sign is the
+     * xor of the operands' signs, so the division sequences are skipped when
+     * m == 0 and the ranges below keep every intermediate finite; anything
+     * else is computed as written (bit-identical either way). */
+    static __device__ __forceinline__ R zero_xor(long long s) { return __longlong_as_double(s & (1LL << 63)); }
+    static __device__ __forceinline__ R e3_term(R num, R J, R yJ, int ok, R m)
+    {
+        if (m == 0 && ok && fabs(num) <= 0x1p900)
+            return zero_xor(__double_as_longlong(num) ^ __double_as_longlong(J) ^ __double_as_longlong(m));
+        return divk(num, J, yJ, ok) * m;
+    }
+    /* T > 1e-6 here (SWEHR.c:1368) */
+    static __device__ __forceinline__ R e4_term(R A, R T, R F, R e, R m)
+    {
+        const R ae = fabs(e);
+        if (m == 0 && fabs(A) <= 0x1p500 && fabs(F) <= 0x1p100 && ae >= 0x1p-300 && ae <= 0x1p300)
+            return zero_xor(__double_as_longlong(A) ^ __double_as_longlong(T) ^ __double_as_longlong(F) ^
+                            __double_as_longlong(e) ^ __double_as_longlong(m));
+        return div(div(A, T) * F, e) * m;
+    }
     /* settling velocity of Cao 2006 (SWEHR.c:435): sqrt(A^2 + c) - A, in the
      * reference's operation order */
     static __device__ __forceinline__ R settle(R A, R A2, R c) { return sqrtp(A2 + c) - A; }
@@ -166,6 +189,8 @@ struct PolicyF32 {
     static __device__ __forceinline__ R divz(R a, R b) { return div(a, b); }
     static __device__ __forceinline__ R sqrtz(R x) { return sqrtp(x); }
     static __device__ __forceinline__ R divk(R a, R c, R, int) { return div(a, c); }
+    static __device__ __forceinline__ R e3_term(R num, R J, R yJ, int ok, R m) { return divk(num, J, yJ, ok) * m; }
+    static __device__ __forceinline__ R e4_term(R A, R T, R F, R e, R m) { return div(div(A, T) * F, e) * m; }
     static __device__ __forceinline__ R qnan() { return __int_as_float(0x7fc00000); }
     /* settling velocity sqrt(A^2 + c) - A rewritten as c / (sqrt(A^2 + c) + A):
      * equal in exact arithmetic, but for fine classes (d = 2 um: A = 8.37,
@@ -1106,9 +1131,9 @@ __device__ __forceinline__ void tile_cell(const DevParams &P, const SetV<RS> &sr
             if (swash && !debris) {
                 if (totm0 > R(1e-8) && Mk0r > R(1e-8)) E2 = PP::div(Hs * Mk0r, totm0) * K.ad * Rc;
                 if (deepv) E2 = E2 * depthfac;
-                E3 = PP::divk((1 - Hs) * K.pf[k] * K.F, K.J, (R)P.inv_J, P.divk_ok) * (h0v > K.ds[k] ? E3b : R(0));
+                E3 = PP::e3_term((1 - Hs) * K.pf[k] * K.F, K.J, (R)P.inv_J, P.divk_ok, h0v > K.ds[k] ? E3b : R(0));
                 if (totm0 > R(1e-6) && Mk0r > 0)
-                    E4 = PP::div(PP::div(K.one_m_bb * Hs * Mk0r, totm0) * K.F, e4den) * (h0v > K.ds[k] ? E4b : R(0));
+                    E4 = PP::e4_term(K.one_m_bb * Hs * Mk0r, totm0, K.F, e4den, h0v > K.ds[k] ? E4b : R(0));
             }
             if (!debris) {
                 VF = PP::settle(K.a13[k], K.a13sq[k], K.c109s * gz * K.ds[k]);
@@ -1166,7 +1191,7 @@ __device__ __forceinline__ void tile_cell(const DevParams &P, const SetV<RS> &sr
         for (int k = 0; k < MAXS; k++) {
             if (k >= S) break;
             const R uk = kSlot ? (R)Uslot[k * hps] : Ureg[kSlot ? 0 : k];
-            totsed += PP::divk(PP::div(uk, h), rhos, (R)P.inv_rhos, P.divk_ok);
+            totsed += PP::divk(PP::divz(uk, h), rhos, (R)P.inv_rhos, P.divk_ok);
             dst.U[k * pl + q] = (RS)uk;
             if (L.stage_m) dst.M[k * pl + q] = celld[(CD_M + k) * T_I * T_J + cs];
         }
