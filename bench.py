@@ -53,16 +53,35 @@ def algo_bytes_mixed(S: int) -> int:
     return 2 * (4 * (5 + S) + 8 * (2 + S)) + 4
 
 
-def profiled_traffic(summary: str):
-    """DRAM bytes per cell-step of a kernel, from its committed ncu summary
-    (dram__bytes_read.sum + dram__bytes_write.sum of one captured launch on
-    a 1024^2 case, divided by its cells; per-cell traffic is size
-    independent once the state is far larger than L2)."""
+def profiled(summary: str, key: str = "traffic_bytes_per_cell_step"):
+    """A per-cell figure of a kernel from its committed ncu summary: DRAM
+    bytes per cell-step (dram__bytes_read.sum + dram__bytes_write.sum of one
+    captured launch on a 1024^2 case, divided by its cells; per-cell traffic
+    is size independent once the state is far larger than L2), or FP64
+    operations per cell-step (2 x DFMA + DMUL + DADD thread instructions)."""
     path = os.path.join(ROOT, "profiles", summary)
     try:
         for line in open(path):
-            if line.startswith("traffic_bytes_per_cell_step:"):
+            if line.startswith(key + ":"):
                 return float(line.split(":")[1])
+    except OSError:
+        pass
+    return None
+
+
+def profiled_traffic(summary: str):
+    return profiled(summary)
+
+
+def fp64_peak():
+    """The FP64 pipe's ceiling on this GPU in TFLOP/s, measured now by
+    swehr_probe_fp64_peak (independent FMA chains at full occupancy)."""
+    import ctypes
+    try:
+        lib = ctypes.CDLL(os.path.join(ROOT, "swehr_b200", "libswehr_probe.so"))
+        v = ctypes.c_double()
+        if lib.swehr_probe_fp64_peak(ctypes.byref(v)) == 0 and v.value > 0:
+            return v.value
     except OSError:
         pass
     return None
@@ -209,7 +228,10 @@ def ensemble_leg(args, ranks):
     mine = shard([c.cells() for c in all_cases], ranks.world)[ranks.rank]
     cases = [all_cases[k] for k in mine]
     cells = sum(c.cells() for c in all_cases)
-    cap = 64 + args.ens_warmup + args.ens_steps   # pool steps every scenario runs (the tuner's included)
+    # pool steps every scenario runs: the tuner's (up to 2 shapes x 8 grids x
+    # 3 rounds x 4 steps), the warm-up and the timed ones, so that every
+    # scenario is still running through the whole timed window
+    cap = 256 + args.ens_warmup + args.ens_steps
     every = max(1, len(all_cases) // 8)
     subset = [i for i, k in enumerate(mine) if k % every == 0 and k // every < 8]
     names = ("h", "totsed", "sed")
@@ -231,6 +253,7 @@ def ensemble_leg(args, ranks):
             pool.run(-1)
             keep[label] = [scs[k].fields(names) for k in subset]
             out[label] = {"value": cs / (dev_ms / 1e3), "unit": "cell-steps/s", "pool_steps": int(st.pool_steps),
+                          "tuner_steps": int(tu.pool_steps), "scenario_steps_timed": cs / max(cells, 1),
                           "device_ms": dev_ms, "ms_per_pool_step": dev_ms / max(st.pool_steps, 1),
                           "grid_wave": int(tu.grid_wave), "grid_update": int(tu.grid_update),
                           "tile": f"{int(tu.tile_i)}x{int(tu.tile_j)}",
@@ -381,16 +404,20 @@ def main():
     S = case.sclass
     cells = case.cells()
 
-    def window(prw, B):
-        """throughput and update-kernel roofline of a timed window"""
+    def window(prw, B, prof):
+        """throughput and update-kernel roofline of a timed window (prof: the
+        committed ncu summary of the same kernel in the same flow state)"""
         ms = max_over_ranks(prw.device_ms)
         n = max(int(prw.steps_this_call), 1)
         upd = prw.kernel_ms / n
         ach = B * cells / (upd / 1e3) / 1e9 if upd > 0 else None
         first = int(prw.steps) - n
+        tb, ff = profiled(prof), profiled(prof, "fp64_flop_per_cell_step")
         return {"steps": f"{first}..{int(prw.steps)}", "value": world * cells * n / (ms / 1e3),
                 "unit": "cell-steps/s", "ms_per_step": ms / n, "update_ms_avg": upd, "achieved_gbs": ach,
-                "frac": (ach / hbm_peak()[0]) if ach else None}
+                "frac": (ach / hbm_peak()[0]) if ach else None, "traffic": tb * cells if tb else None,
+                "fp64_tflops": ff * cells / (upd / 1e3) / 1e12 if (ff and upd > 0) else None,
+                "profile": "profiles/" + prof}
 
     def timed_run(precision, clocks=None):
         """W warm-up steps, K timed steps; then, untimed, on to the steady
@@ -431,7 +458,7 @@ def main():
         vm = world * cells * prm.steps_this_call / (em / 1e3)
         um = prm.kernel_ms / max(prm.steps_this_call, 1)
         Bm = algo_bytes_mixed(S)
-        tm = profiled_traffic("k_update_tile_f32_fractal1024.md")
+        tm = profiled_traffic("k_update_tile_f32_dry_fractal1024.md")
         mixed = {"value": vm, "unit": "cell-steps/s", "ms_per_step": em / max(prm.steps_this_call, 1),
                  "steps": int(prm.steps_this_call), "gpu_launches": int(prm.kernel_launches),
                  "over_fp64": vm / value,
@@ -443,7 +470,7 @@ def main():
                  "dtype": "f32 bulk; f64 z, infiltration, deposited mass, budgets",
                  "error_bar": "<=1e-4 relative L-inf on depth and concentration vs FP64 (tests/test_gpu_mixed.py)"}
         if stm is not None:
-            mixed["steady"] = window(stm, algo_bytes_mixed(S))
+            mixed["steady"] = window(stm, algo_bytes_mixed(S), "k_update_tile_f32_wet_fractal1024.md")
 
     # end-to-end through the C ABI from host buffers: create (H2D of every
     # input) + the same steps + D2H of the fields SWEHR.c writes at the end
@@ -454,7 +481,9 @@ def main():
         barrier()
         t0 = time.perf_counter()
         s2 = Simulation(case)
+        ta = time.perf_counter()
         s2.advance(max_steps=args.warmup + args.steps)
+        tb = time.perf_counter()
         out = s2.fields(("h", "hu", "hv", "z", "totm", "totsed", "vel", "maxvel", "maxdepth"))
         out["U1"] = s2.field("U", 1)
         t1 = time.perf_counter()
@@ -466,9 +495,10 @@ def main():
         e2e = {"value": e2e_val, "unit": "cell-steps/s", "h2d_bytes_per_step": h2d / n_e2e,
                "d2h_bytes_per_step": d2h / n_e2e,
                "scope": "swehr_create + swehr_advance + swehr_read_field of the ten result grids SWEHR.c writes "
-                        "(depth uh vh topoout ch m c vel maxvel maxdepth), host buffers"}
+                        "(depth uh vh topoout ch m c vel maxvel maxdepth), host buffers",
+               "phases_s": {"create": ta - t0, "advance": tb - ta, "read": t1 - tb}}
 
-    steady = window(st64, algo_bytes_f64(S)) if st64 is not None else None
+    steady = window(st64, algo_bytes_f64(S), "k_update_tile_f64_wet_fractal1024.md") if st64 is not None else None
     if steady is not None and mixed is not None and mixed.get("steady"):
         mixed["steady"]["over_fp64"] = mixed["steady"]["value"] / steady["value"]
 
@@ -503,7 +533,15 @@ def main():
         B = algo_bytes_f64(S)
         upd_ms = kernel_ms / max(steps_done, 1)
         achieved = B * cells / (upd_ms / 1e3) / 1e9 if upd_ms > 0 else None
-        tb = profiled_traffic("k_update_tile_f64_fractal1024.md")
+        tb = profiled_traffic("k_update_tile_f64_dry_fractal1024.md")
+        fpk = fp64_peak()
+        ff = profiled("k_update_tile_f64_dry_fractal1024.md", "fp64_flop_per_cell_step")
+        fach = ff * cells / (upd_ms / 1e3) / 1e12 if (ff and upd_ms > 0) else None
+        fp64 = {"peak_tflops": fpk, "peak_kind": "measured now (FMA chains, swehr_b200/csrc/swehr_probe.cu)",
+                "flop_per_cell_step": ff, "achieved_tflops": fach,
+                "frac": (fach / fpk) if (fach and fpk) else None,
+                "flop_source": "ncu thread-instruction counters of the same kernel and window "
+                               "(profiles/k_update_tile_f64_dry_fractal1024.md)"}
         traffic = tb * cells if tb else None
         line = {
             "metric": "cell-steps/s", "value": value, "unit": "cell-steps/s", "n_gpus": world,
@@ -518,7 +556,10 @@ def main():
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": (achieved / peak) if achieved else None, "traffic": traffic,
                          "peak_kind": peak_kind, "kernel": "k_update (FP64)",
-                         "algo_bytes_per_cell_step": B, "update_ms_avg": upd_ms},
+                         "algo_bytes_per_cell_step": B, "update_ms_avg": upd_ms, "fp64": fp64,
+                         "limiter": "issue and dependency latency: neither HBM nor the FP64 pipe is saturated "
+                                    "(ncu: DRAM, FP64 pipe and issue-active fractions and stall reasons in "
+                                    "profiles/k_update_tile_f64_*_fractal1024.md)"},
             "cpu_baseline": cpu,
             "e2e": e2e,
             "steady_state": steady,
