@@ -96,9 +96,11 @@ def hbm_peak():
 
 
 class ClockSampler:
-    """nvidia-smi clock samples during the timed region."""
+    """nvidia-smi clock samples (every 20 ms) kept only where their timestamps
+    fall inside the timed windows: the sampler starts before the simulation
+    is created, so it is producing samples when the short timed regions run."""
 
-    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+    FIELDS = ("timestamp,index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
               "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
               "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
 
@@ -106,14 +108,19 @@ class ClockSampler:
         self.path = tempfile.mktemp(prefix="clocks_", suffix=".csv")
         self.idx = gpu_index
         self.proc = None
+        self.windows = []
 
     def start(self):
         try:
             self.proc = subprocess.Popen(
                 ["nvidia-smi", f"--id={self.idx}", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
-                 "-lms", "200"], stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+                 "-lms", "20"], stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
         except Exception:
             self.proc = None
+
+    def window(self, t0: float, t1: float):
+        """a timed region, host wall-clock seconds (time.time()) around it"""
+        self.windows.append((t0, t1))
 
     def stop(self):
         if self.proc is None:
@@ -123,29 +130,37 @@ class ClockSampler:
             self.proc.wait(timeout=5)
         except Exception:
             self.proc.kill()
-        sm, smax, reasons = [], [], set()
+        import datetime
+        rows = []
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
         try:
             for line in open(self.path):
                 p = [x.strip() for x in line.split(",")]
-                if len(p) < 9:
+                if len(p) < 10:
                     continue
                 try:
-                    sm.append(float(p[1]))
-                    smax.append(float(p[2]))
+                    ts = datetime.datetime.strptime(p[0], "%Y/%m/%d %H:%M:%S.%f").timestamp()
+                    rows.append((ts, float(p[2]), float(p[3]),
+                                 {n for n, v in zip(names, p[6:10]) if v.lower() in ("active", "1", "yes")}))
                 except ValueError:
                     continue
-                for n, v in zip(names, p[5:9]):
-                    if v.lower() in ("active", "1", "yes"):
-                        reasons.add(n)
         except FileNotFoundError:
             pass
         try:
             os.unlink(self.path)
         except OSError:
             pass
-        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(smax) if smax else None,
-                "reasons": sorted(reasons), "samples": len(sm)}
+        inside = [r for r in rows if any(a <= r[0] <= b for a, b in self.windows)]
+        sel = inside
+        if not sel and rows and self.windows:
+            # no sample landed inside (windows of ~0.1 s): the samples nearest to them
+            d = lambda r: min(min(abs(r[0] - a), abs(r[0] - b)) for a, b in self.windows)
+            sel = sorted(rows, key=d)[:3]
+        sm = [r[1] for r in sel]
+        reasons = set().union(*[r[3] for r in sel]) if sel else set()
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(r[2] for r in sel) if sel else None,
+                "reasons": sorted(reasons), "samples": len(sel), "samples_inside_windows": len(inside),
+                "windows_s": [round(b - a, 3) for a, b in self.windows]}
 
 
 def bench_workload(args):
@@ -423,24 +438,30 @@ def main():
         """W warm-up steps, K timed steps; then, untimed, on to the steady
         window (the domain wets up over the first ~1000 steps: dry at step 25,
         58 % wet at 600, wet everywhere by 1000) and K more timed steps there."""
+        if clocks:
+            clocks.start()
         sim = Simulation(case, precision=precision)
         sim.advance(max_steps=args.warmup)
         barrier()
-        if clocks:
-            clocks.start()
         sim.set_timing(True)
+        t0 = time.time()
         pr = sim.advance(max_steps=args.steps)
+        if clocks:
+            clocks.window(t0, time.time())
         sim.set_timing(False)
-        clk = clocks.stop() if clocks else None
         barrier()
         steady = None
         if args.steady_at > args.warmup + args.steps:
             sim.advance(max_steps=args.steady_at - (args.warmup + args.steps))
             barrier()
             sim.set_timing(True)
+            t0 = time.time()
             steady = sim.advance(max_steps=args.steps)
+            if clocks:
+                clocks.window(t0, time.time())
             sim.set_timing(False)
             barrier()
+        clk = clocks.stop() if clocks else None
         sim.close()
         return pr, clk, steady
 

@@ -291,6 +291,64 @@ int swehr_pool_stats_get(swehr_pool *pool, swehr_pool_stats *stats);
 
 void swehr_pool_destroy(swehr_pool *pool);
 
+/* ---- One domain split into row slabs (several devices, or several slabs of
+ * one device).  No counterpart in the reference, whose loop body
+ * (SWEHR.c:808-1591) runs serially over the whole grid; these replace the
+ * same loop body for the rows row_lo..row_hi of the domain.  A step of row i
+ * reads rows i-1..i+1 of the previous state and i-2..i+2 of the topography
+ * (SWEHR.c:1135, 1203, 1243-1312), and the time step is one maximum over
+ * every face of the grid (SWEHR.c:1408).  So a slab context holds its rows
+ * plus up to two rows of each neighbour, updates only its own rows, and one
+ * step is:
+ *   swehr_slab_wave on every slab          largest wave speed of its faces
+ *   maximum of those speeds, written back  (swehr_slab_smax_ptr: 8 bytes of
+ *                                           device memory per slab, the bit
+ *                                           pattern of a non-negative double,
+ *                                           so an unsigned 64-bit max-reduce
+ *                                           is the max of the speeds)
+ *   swehr_slab_update on every slab        time step and update of its rows
+ *   swehr_slab_pack / copy / unpack        its two edge rows of every state
+ *                                           plane and of the new topography
+ *                                           into the neighbours' halo rows
+ * All calls are asynchronous on the slab's stream (swehr_slab_stream).
+ * Whole-domain inputs and parameters are passed to swehr_slab_create, which
+ * keeps the slab's rows.  Budgets, stage rows, interior solid cells and the
+ * pool are not available for slabs (SWEHR_INVALID).  The slab's context
+ * works with swehr_read_field (its local rows, halo rows included),
+ * swehr_destroy and the calls below, not with swehr_advance. */
+int swehr_slab_create(const swehr_params *p, const swehr_inputs *in, int precision, int row_lo, int row_hi,
+                      swehr_ctx **out);
+
+/* the slab's local rows: halo_lo rows above its own rows, then row_hi - row_lo + 1
+ * own rows, then halo_hi rows (halo_lo, halo_hi in 0..2) */
+int swehr_slab_rows(swehr_ctx *ctx, int *halo_lo, int *own, int *halo_hi);
+
+int swehr_slab_wave(swehr_ctx *ctx);
+int swehr_slab_smax_ptr(swehr_ctx *ctx, void **dev_ptr);
+int swehr_slab_update(swehr_ctx *ctx);
+
+/* Halo exchange buffers, one per side (0: toward row 1, 1: toward row nx),
+ * each `bytes` long: pack fills both send buffers from the rows the step
+ * just wrote, unpack writes both receive buffers into the halo rows.  A side
+ * without a neighbour is neither packed nor unpacked. */
+int swehr_slab_buffers(swehr_ctx *ctx, int side, void **send, void **recv, size_t *bytes);
+int swehr_slab_pack(swehr_ctx *ctx);
+int swehr_slab_unpack(swehr_ctx *ctx);
+
+/* the slab's cudaStream_t */
+int swehr_slab_stream(swehr_ctx *ctx, void **stream);
+
+/* wait for the slab's stream and report t, steps, the last dt and Courant
+ * number, status and done (no more steps: t >= tend or a CFL error) */
+int swehr_slab_progress(swehr_ctx *ctx, swehr_progress *pr);
+
+/* For slabs driven by one host thread: max-reduce the n slabs' wave speeds
+ * into every slab, and copy slab a's send buffer of `side` into the
+ * neighbour b's receive buffer (peer copy across devices); both order
+ * themselves after the slabs' earlier work and before their later work. */
+int swehr_slab_reduce_local(swehr_ctx *const *ctxs, int n);
+int swehr_slab_copy_halo(swehr_ctx *a, int side, swehr_ctx *b);
+
 #ifdef __cplusplus
 }
 #endif

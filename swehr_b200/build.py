@@ -31,6 +31,7 @@ SOURCES = [
     ("swehr_cfl_noalloc.cu", ["--fmad=false"]),
     ("swehr_batch16_f64.cu", ["--fmad=false"]),
     ("swehr_batch16_f32.cu", []),
+    ("swehr_slab.cu", ["--fmad=false"]),
 ]
 
 

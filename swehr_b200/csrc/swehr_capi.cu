@@ -215,6 +215,10 @@ static void make_devparams(const swehr_params *p, const swehr_inputs *in, const 
     for (int m = 0; m < 6; m++) { P.xpoint[m] = p->xpoint[m]; P.ypoint[m] = p->ypoint[m]; }
     P.has_ks = in->ks != nullptr;
     P.has_solid = in->solid != nullptr;
+    P.own_lo = 1;
+    P.own_hi = p->nx;
+    P.row0 = 0;
+    P.slab = 0;
     P.plane = L.plane;
     P.dx = p->dx; P.oneoverdx = 1 / p->dx; P.half_odx = 0.5 * P.oneoverdx; P.tend = p->tend; P.rint = p->rint;
     P.stageint = p->stageint;
@@ -463,6 +467,7 @@ static void destroy_ctx(swehr_ctx *c)
         free(c->h_ctl);
     } else {
         if (c->mem) cudaFree(c->mem);
+        if (c->d_halo) cudaFree(c->d_halo);
         if (c->h_ctl) cudaFreeHost(c->h_ctl);
         if (c->stream) cudaStreamDestroy(c->stream);
     }
@@ -675,6 +680,7 @@ extern "C" int swehr_advance(swehr_ctx *c, double t_stop, int64_t max_steps, swe
 {
     if (!c) return set_err(SWEHR_INVALID, "NULL ctx");
     if (c->pooled) return set_err(SWEHR_INVALID, "a pooled scenario is stepped by its pool");
+    if (c->slab) return set_err(SWEHR_INVALID, "a slab is stepped by the swehr_slab_* calls");
     auto wall0 = std::chrono::steady_clock::now();
     /* read the control block, arm it */
     CK(cudaMemcpyAsync(c->h_ctl, c->d_ctl, sizeof(Ctl), cudaMemcpyDeviceToHost, c->stream));

@@ -51,6 +51,11 @@ struct swehr_ctx {
     int64_t stagecap = 0;
     double water_init = 0;
     double sed_init[SWEHR_MAX_CLASSES] = {};
+    /* a slab of a split domain (swehr_slab_create): halo rows held on each
+     * side, and the device buffers send[2] then recv[2], halo_bytes each */
+    int slab = 0, halo_lo = 0, halo_hi = 0;
+    char *d_halo = nullptr;
+    size_t halo_bytes = 0;
 };
 
 /* record an error message for swehr_last_error() and return code */

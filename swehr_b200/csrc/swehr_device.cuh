@@ -43,6 +43,12 @@ struct DevParams {
     int32_t bndry[4];
     int32_t outlet_row, npoints, xpoint[6], ypoint[6];
     int32_t has_ks, has_solid;   /* per-cell Ks plane; interior solid mask (SOLID, SWEHR.c:597) */
+    /* rows this context updates (1-based, local): 1..nx for a whole domain;
+     * a slab of a larger domain holds up to two neighbour rows on each inner
+     * side that it reads but does not update.  row0: global row of local row
+     * 0 (positions of the moving storm).  slab: the CFL time step waits for
+     * the largest wave speed over every slab (k_slab_finalize). */
+    int32_t own_lo, own_hi, row0, slab;
     int64_t plane;        /* doubles per plane (>= nx*pitch, multiple of 32) */
     double dx, oneoverdx, half_odx, tend, rint, stageint;
     double g, hfilm, hfx10, rhos, rhow, rho0, porod, invporo;

@@ -101,9 +101,16 @@ int configure_step_f32(const DevParams &P, int num_sms, StepConfig &cfg);
 int launch_step_f64(const DevParams &P, const BufsT<double> &B, Ctl *ctl, const double *rain, double *partials,
                     double *stage, double *saveflow, const TmaMaps &tm, const StepConfig &cfg, cudaStream_t s,
                     cudaEvent_t ev0, cudaEvent_t ev1);
-/* the update kernel's tile loads through tensor maps (FP64 form, one
- * domain): whether the driver offers the encoder, and the maps of a
- * simulation's planes (0 when all were encoded) */
+/* the two passes of a step separately (slabs of a split domain) */
+int launch_wave_f64(const DevParams &P, const BufsT<double> &B, Ctl *ctl, const StepConfig &cfg, cudaStream_t s);
+int launch_wave_f32(const DevParams &P, const BufsT<float> &B, Ctl *ctl, const StepConfig &cfg, cudaStream_t s);
+int launch_update_f64(const DevParams &P, const BufsT<double> &B, Ctl *ctl, const double *rain, double *partials,
+                      double *stage, double *saveflow, const TmaMaps &tm, const StepConfig &cfg, cudaStream_t s);
+int launch_update_f32(const DevParams &P, const BufsT<float> &B, Ctl *ctl, const double *rain, double *partials,
+                      double *stage, double *saveflow, const TmaMaps &tm, const StepConfig &cfg, cudaStream_t s);
+/* the update kernel's tile loads through tensor maps (one domain): whether
+ * the driver offers the encoder, and the maps of a simulation's planes (0
+ * when all were encoded) */
 int tma_available();
 int encode_tma_f64(const DevParams &P, const BufsT<double> &B, TmaMaps &tm);
 int encode_tma_f32(const DevParams &P, const BufsT<float> &B, TmaMaps &tm);

@@ -262,6 +262,24 @@ struct FormLauncher {
         if (ev1) cudaEventRecord(ev1, s);
         return (int)cudaGetLastError();
     }
+
+    /* the two passes of a step one at a time (a slab of a split domain takes
+     * the largest wave speed over every slab between them) */
+    static int launch_wave(const DevParams &P, const BufsT<RS> &B, Ctl *ctl, const StepConfig &cfg, cudaStream_t s)
+    {
+        void *wargs[] = {(void *)&P, (void *)&B, (void *)&ctl};
+        cudaLaunchKernel(cfg.fn_wave, dim3(cfg.grid_wave), dim3(TILE_THREADS), wargs, cfg.smem_wave, s);
+        return (int)cudaGetLastError();
+    }
+
+    static int launch_update(const DevParams &P, const BufsT<RS> &B, Ctl *ctl, const double *rain, double *partials,
+                             double *stage, double *saveflow, const TmaMaps &tm, const StepConfig &cfg, cudaStream_t s)
+    {
+        void *args[] = {(void *)&P, (void *)&B, (void *)&ctl, (void *)&rain, (void *)&partials, (void *)&stage,
+                        (void *)&saveflow, (void *)&tm};
+        cudaLaunchKernel(cfg.fn_update, dim3(cfg.grid_update), dim3(TILE_THREADS), args, cfg.smem_update, s);
+        return (int)cudaGetLastError();
+    }
 };
 
 }  // inline namespace SWEHR_TILE_NS

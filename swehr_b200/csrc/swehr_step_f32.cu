@@ -14,6 +14,17 @@ int configure_step_f32(const DevParams &P, int num_sms, StepConfig &cfg)
     return FormLauncher<PolicyF32, float>::configure(P, num_sms, cfg);
 }
 
+int launch_wave_f32(const DevParams &P, const BufsT<float> &B, Ctl *ctl, const StepConfig &cfg, cudaStream_t s)
+{
+    return FormLauncher<PolicyF32, float>::launch_wave(P, B, ctl, cfg, s);
+}
+
+int launch_update_f32(const DevParams &P, const BufsT<float> &B, Ctl *ctl, const double *rain, double *partials,
+                      double *stage, double *saveflow, const TmaMaps &tm, const StepConfig &cfg, cudaStream_t s)
+{
+    return FormLauncher<PolicyF32, float>::launch_update(P, B, ctl, rain, partials, stage, saveflow, tm, cfg, s);
+}
+
 int init_gz_f32(const DevParams &P, const BufsT<float> &B, int64_t n, cudaStream_t s)
 {
     return FormLauncher<PolicyF32, float>::init_gz(P, B, n, s);

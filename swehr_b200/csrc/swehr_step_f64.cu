@@ -27,6 +27,17 @@ int configure_step_f64(const DevParams &P, int num_sms, StepConfig &cfg)
     return FormLauncher<PolicyF64, double>::configure(P, num_sms, cfg);
 }
 
+int launch_wave_f64(const DevParams &P, const BufsT<double> &B, Ctl *ctl, const StepConfig &cfg, cudaStream_t s)
+{
+    return FormLauncher<PolicyF64, double>::launch_wave(P, B, ctl, cfg, s);
+}
+
+int launch_update_f64(const DevParams &P, const BufsT<double> &B, Ctl *ctl, const double *rain, double *partials,
+                      double *stage, double *saveflow, const TmaMaps &tm, const StepConfig &cfg, cudaStream_t s)
+{
+    return FormLauncher<PolicyF64, double>::launch_update(P, B, ctl, rain, partials, stage, saveflow, tm, cfg, s);
+}
+
 int init_gz_f64(const DevParams &P, const BufsT<double> &B, int64_t n, cudaStream_t s)
 {
     return FormLauncher<PolicyF64, double>::init_gz(P, B, n, s);

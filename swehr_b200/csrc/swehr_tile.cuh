@@ -288,11 +288,12 @@ struct TileCoord {
     int i0, j0;
 };
 
+/* tiles cover the rows the context updates (own_lo..own_hi) */
 __device__ __forceinline__ TileCoord tile_coord(const DevParams &P, int64_t tile)
 {
     const int ntj = (P.ny + T_J - 1) / T_J;
     TileCoord t;
-    t.i0 = (int)(tile / ntj) * T_I + 1;
+    t.i0 = (int)(tile / ntj) * T_I + P.own_lo;
     t.j0 = (int)(tile % ntj) * T_J + 1;
     return t;
 }
@@ -778,11 +779,13 @@ __global__ void __launch_bounds__(TILE_THREADS, PP::kWaveMinBlocks) k_wave_cells
     double inh = 0, inhv = 0, insed = 0;
     if (P.inflow) inflow_ghost(t, inh, inhv, insed);
     /* cells in i-major order, j contiguous; (i, j) advanced by the stride */
-    const int64_t total = (int64_t)P.nx * P.ny;
+    /* the cells of the rows this context updates; a face belongs to the
+     * row of its lower (left) cell, face 1/2 to row 1 */
+    const int64_t total = (int64_t)(P.own_hi - P.own_lo + 1) * P.ny;
     const int64_t stride = (int64_t)gridDim.x * blockDim.x;
     const int64_t c0 = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     const int si = (int)(stride / P.ny), sj = (int)(stride - (int64_t)si * P.ny);
-    int i = (int)(c0 / P.ny) + 1, j = (int)(c0 - (int64_t)(i - 1) * P.ny) + 1;
+    int i = (int)(c0 / P.ny) + P.own_lo, j = (int)(c0 - (int64_t)(i - P.own_lo) * P.ny) + 1;
     R smax = 0;
     for (int64_t c = c0; c < total; c += stride) {
         const R s = wave_cell<PP, RS>(P, src, i, j, (R)inh, (R)inhv, P.has_solid ? B.solid : nullptr);
@@ -798,7 +801,12 @@ __global__ void __launch_bounds__(TILE_THREADS, PP::kWaveMinBlocks) k_wave_cells
         last = (atomicAdd(&ctl->wave_ticket, 1u) == gridDim.x - 1);
     }
     __syncthreads();
-    if (last && threadIdx.x == 0) wave_finalize(P, ctl);
+    if (last && threadIdx.x == 0) {
+        if (P.slab)
+            ctl->wave_ticket = 0u;       /* dt waits for the largest speed over every slab */
+        else
+            wave_finalize(P, ctl);
+    }
 }
 
 /* the gz plane of the set step n reads, from its previous-step topography
@@ -892,7 +900,7 @@ template <class PP>
 __device__ __forceinline__ typename PP::R storm_r(const DevParams &P, double t, int i, int j)
 {
     typedef typename PP::R R;
-    const double x = ((double)i - 0.5) * P.dx - (P.storm_x0 + P.storm_vx * t);
+    const double x = ((double)(i + P.row0) - 0.5) * P.dx - (P.storm_x0 + P.storm_vx * t);
     const double y = ((double)j - 0.5) * P.dx - (P.storm_y0 + P.storm_vy * t);
     const double r2 = (x * x + y * y) / P.storm_r2;
     return (R)P.storm_peak * PP::exp(R(-0.5 * r2));
@@ -943,7 +951,7 @@ __device__ __forceinline__ void tile_cell(const DevParams &P, const SetV<RS> &sr
     const RealC<R> &K = kc<R>(P);
     const int ti = threadIdx.x / T_J, tj = threadIdx.x % T_J;
     const int i = tc.i0 + ti, j = tc.j0 + tj;
-    if (i > P.nx || j > P.ny) return;
+    if (i > P.own_hi || j > P.ny) return;
     const int64_t pl = P.plane;
     const int64_t q = cidx(P, i, j);
     if (P.has_solid && solid[q]) {
@@ -1525,7 +1533,7 @@ __global__ void __launch_bounds__(TILE_THREADS, PP::kMinBlocks) k_update_tile(co
     const double Rr = P.storm ? 0.0 : rain_at(P, rain, t);
     Acc2<MAXS, BUDGET> acc;
     acc_zero(acc);
-    const int64_t ntiles = (int64_t)((P.nx + T_I - 1) / T_I) * ((P.ny + T_J - 1) / T_J);
+    const int64_t ntiles = (int64_t)((P.own_hi - P.own_lo + T_I) / T_I) * ((P.ny + T_J - 1) / T_J);
     for (int64_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x)
         update_tile<PP, RS, MAXS, BUDGET, TMA, NS>(P, B, n, t, dt, Rr, tile_coord(P, tile), smb, L, acc, &tm, &tma_bar,
                                                &tma_phase, ctl);

@@ -75,6 +75,25 @@ def load() -> C.CDLL:
     L.swehr_pool_stats_get.restype = i32
     L.swehr_pool_stats_get.argtypes = [vp, vp]
     L.swehr_pool_destroy.argtypes = [vp]
+    L.swehr_slab_create.restype = i32
+    L.swehr_slab_create.argtypes = [vp, vp, i32, i32, i32, C.POINTER(vp)]
+    L.swehr_slab_rows.restype = i32
+    L.swehr_slab_rows.argtypes = [vp, C.POINTER(i32), C.POINTER(i32), C.POINTER(i32)]
+    for n in ("swehr_slab_wave", "swehr_slab_update", "swehr_slab_pack", "swehr_slab_unpack"):
+        getattr(L, n).restype = i32
+        getattr(L, n).argtypes = [vp]
+    L.swehr_slab_smax_ptr.restype = i32
+    L.swehr_slab_smax_ptr.argtypes = [vp, C.POINTER(vp)]
+    L.swehr_slab_buffers.restype = i32
+    L.swehr_slab_buffers.argtypes = [vp, i32, C.POINTER(vp), C.POINTER(vp), C.POINTER(C.c_size_t)]
+    L.swehr_slab_stream.restype = i32
+    L.swehr_slab_stream.argtypes = [vp, C.POINTER(vp)]
+    L.swehr_slab_progress.restype = i32
+    L.swehr_slab_progress.argtypes = [vp, vp]
+    L.swehr_slab_reduce_local.restype = i32
+    L.swehr_slab_reduce_local.argtypes = [C.POINTER(vp), i32]
+    L.swehr_slab_copy_halo.restype = i32
+    L.swehr_slab_copy_halo.argtypes = [vp, i32, vp]
     if L.swehr_params_size() != C.sizeof(SwehrParams):
         raise ImportError(f"swehr_params size mismatch: C {L.swehr_params_size()} vs ctypes {C.sizeof(SwehrParams)}")
     _lib = L
@@ -289,3 +308,95 @@ class Pool:
             self.close()
         except Exception:
             pass
+
+
+class SlabDomain:
+    """One domain split into slabs of whole rows (swehr_slab_*), every slab
+    driven by this process: a step is the wave pass of every slab, the
+    largest wave speed over all of them, every slab's update, and the halo
+    rows moved between neighbours by device copies (peer copies when the
+    slabs sit on different devices).  devices: the device of each slab
+    (default: the current one for all)."""
+
+    def __init__(self, case, slabs: int, precision: int = FP64, devices=None):
+        from .slabs import plan
+        self.L = load()
+        self.case = case
+        self._in = CaseInputs(case, False)
+        self.plan = plan(case.nx, slabs)
+        self.ctx = []
+        self.rows = []
+        torch = None
+        if devices is not None:
+            import torch                     # device selection only
+            cur = torch.cuda.current_device()
+        try:
+            for k, s in enumerate(self.plan):
+                if torch is not None:
+                    torch.cuda.set_device(devices[k])
+                c = C.c_void_p()
+                self._check(self.L.swehr_slab_create(C.byref(self._in.params), C.byref(self._in.inputs), precision,
+                                                     s.own[0], s.own[1], C.byref(c)))
+                self.ctx.append(c)
+                lo, own, hi = C.c_int(), C.c_int(), C.c_int()
+                self._check(self.L.swehr_slab_rows(c, C.byref(lo), C.byref(own), C.byref(hi)))
+                self.rows.append((lo.value, own.value, hi.value))
+        finally:
+            if torch is not None:
+                torch.cuda.set_device(cur)
+        self._arr = (C.c_void_p * len(self.ctx))(*[c.value for c in self.ctx])
+
+    def _check(self, st):
+        if st != 0:
+            raise SwehrError(st, self.L.swehr_last_error().decode())
+
+    def step(self, n: int = 1):
+        L, ctx = self.L, self.ctx
+        for _ in range(n):
+            for c in ctx:
+                self._check(L.swehr_slab_wave(c))
+            self._check(L.swehr_slab_reduce_local(self._arr, len(ctx)))
+            for c in ctx:
+                self._check(L.swehr_slab_update(c))
+                self._check(L.swehr_slab_pack(c))
+            for a, b in zip(ctx, ctx[1:]):
+                self._check(L.swehr_slab_copy_halo(a, 1, b))     # a's last own rows -> b's upper halo
+                self._check(L.swehr_slab_copy_halo(b, 0, a))     # b's first own rows -> a's lower halo
+            for c in ctx:
+                self._check(L.swehr_slab_unpack(c))
+
+    def progress(self) -> SwehrProgress:
+        pr = SwehrProgress()
+        for c in self.ctx:
+            self._check(self.L.swehr_slab_progress(c, C.byref(pr)))
+        return pr
+
+    def field(self, name: str, k: int = 0) -> np.ndarray:
+        """the whole domain's field, each slab's own rows"""
+        parts = []
+        for c, (lo, own, hi) in zip(self.ctx, self.rows):
+            out = np.empty((lo + own + hi, self.case.ny))
+            self._check(self.L.swehr_read_field(c, FIELD_NAMES[name], k, out.ctypes.data))
+            parts.append(out[lo:lo + own])
+        return np.concatenate(parts, axis=0)
+
+    def fields(self, names) -> dict:
+        d = {}
+        for n in names:
+            if FIELD_NAMES[n] in PER_CLASS_FIELDS:
+                d[n] = np.stack([self.field(n, k) for k in range(1, self.case.sclass + 1)])
+            else:
+                d[n] = self.field(n)
+        return d
+
+    def close(self):
+        for c in self.ctx:
+            if c:
+                self.L.swehr_destroy(c)
+        self.ctx = []
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()

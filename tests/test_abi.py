@@ -131,3 +131,22 @@ def _has_device():
         return torch.cuda.is_available()
     except Exception:
         return False
+
+
+def test_slab_entry_points_check_arguments_without_device():
+    """Slab rows, budgets and solid masks are refused before any device call."""
+    L = swlib.load()
+    from swehr_b200.lib import CaseInputs
+    case = W.tiny_case(nx=20, ny=9)
+    inp = CaseInputs(case)
+    h = C.c_void_p()
+    for lo, hi in ((0, 5), (3, 21), (4, 4), (2, 10), (1, 19)):
+        # outside 1..nx, a single row, or a neighbour left with one row
+        assert L.swehr_slab_create(C.byref(inp.params), C.byref(inp.inputs), 0, lo, hi, C.byref(h)) == 5, (lo, hi)
+        assert not h.value
+    inb = CaseInputs(case, budget=True)
+    assert L.swehr_slab_create(C.byref(inb.params), C.byref(inb.inputs), 0, 1, 10, C.byref(h)) == 5
+    for f in ("swehr_slab_wave", "swehr_slab_update", "swehr_slab_pack", "swehr_slab_unpack"):
+        assert getattr(L, f)(None) == 5
+    assert L.swehr_slab_copy_halo(None, 0, None) == 5
+    assert L.swehr_slab_reduce_local(None, 0) == 5
