@@ -70,9 +70,13 @@ struct PolicyF64 {
      * inline exp and division sequences) costs more in instruction fetch
      * than unrolling gains (measured: update -4 % rolled) */
     static constexpr bool kRollClasses = true;
-    /* wave pass register-budgeted for 5 CTAs per SM (48 registers): more
-     * loads in flight outweigh a few spills (measured: pass -6 %) */
-    static constexpr int kWaveMinBlocks = 5;
+    /* wave pass: two cells per thread (16-byte loads) at 3 CTAs per SM (80
+     * registers); measured against one cell per thread at 5 CTAs: wet steps
+     * -0.06 ms, early steps +0.03 ms per 4096^2 step */
+    static constexpr int kWaveMinBlocks = 3;
+    /* skip the division of the density-gradient term where the TOTSED
+     * gradient is an exact zero (see tile_cell; measured: early steps -1 %) */
+    static constexpr bool kKnownResults = true;
     static __device__ __forceinline__ R sqrtp(R x) { return sw_sqrt_pow(x); }
     static __device__ __forceinline__ R pow(R x, R y) { return sw_pow(x, y); }
     static __device__ __forceinline__ R exp(R x) { return sw_exp(x); }
@@ -153,8 +157,13 @@ struct PolicyF64 {
 struct PolicyF32 {
     typedef float R;
     static constexpr int kMinBlocks = 3;
+#ifdef SWEHR_F32_ROLLED
+    static constexpr bool kRollClasses = true;
+#else
     static constexpr bool kRollClasses = false;   /* unrolled is 2 % faster here */
-    static constexpr int kWaveMinBlocks = 8;      /* full occupancy, 32 registers, no spills */
+#endif
+    static constexpr int kWaveMinBlocks = 5;      /* 48 registers: four cells per thread without spills */
+    static constexpr bool kKnownResults = false;
     /* sqrt on the SFU, x * rsqrt(x) (~3 ulp): the mixed form's ~25 square
      * roots per cell (wave speeds, gravity, settling, friction) cost a third
      * of the IEEE sequence; +0 for x <= 0 (the reference's pow(x, 0.5) of a
@@ -735,6 +744,106 @@ __device__ __forceinline__ typename PP::R wave_cell(const DevParams &P, const Se
     return wave_cell_g<PP, RS>(P, src, i, j, inh, inhv, (typename PP::R)src.gz[cidx(P, i, j)], solid);
 }
 
+/* V = 16 / sizeof(RS) consecutive elements of a plane with one 16-byte
+ * load (p is 16-byte aligned: the vector starts on a column multiple of V
+ * of a row whose pitch is a multiple of 32), converted to R */
+template <class RS, class R>
+__device__ __forceinline__ void load_vec(const RS *__restrict__ p, R *out)
+{
+    if constexpr (sizeof(RS) == 4) {
+        const float4 a = __ldg(reinterpret_cast<const float4 *>(p));
+        out[0] = (R)a.x; out[1] = (R)a.y; out[2] = (R)a.z; out[3] = (R)a.w;
+    } else {
+        const double2 a = __ldg(reinterpret_cast<const double2 *>(p));
+        out[0] = (R)a.x; out[1] = (R)a.y;
+    }
+}
+
+/* Largest wave speed over the faces of V consecutive cells (i, j0..j0+V-1)
+ * of a row, j0-1 a multiple of V: the same faces and the same operations as
+ * wave_cell_g for each cell (no interior solid cells), with every plane read
+ * V cells per load.  A cell's normal velocity towards its right neighbour in
+ * the vector is that neighbour's own velocity, formed once. */
+template <class PP, class RS>
+__device__ __forceinline__ typename PP::R wave_vec(const DevParams &P, const SetV<RS> &src, int i, int j0,
+                                                   typename PP::R inh, typename PP::R inhv)
+{
+    typedef typename PP::R R;
+    constexpr int V = Cols<RS>::pad;
+    const RealC<R> &K = kc<R>(P);
+    const int64_t q = cidx(P, i, j0);
+    R h[V], hu[V], hv[V], g[V], u[V], v[V], hd[V], hud[V];
+    load_vec<RS, R>(src.h + q, h);
+    load_vec<RS, R>(src.hu + q, hu);
+    load_vec<RS, R>(src.hv + q, hv);
+    load_vec<RS, R>(src.gz + q, g);
+    const bool below = i < P.nx;
+    if (below) {
+        load_vec<RS, R>(src.h + q + P.pitch, hd);
+        load_vec<RS, R>(src.hu + q + P.pitch, hud);
+    }
+    /* the cell after the vector, for the last cell's y face */
+    const int jl = j0 + V;
+    R hn = 0, hvn = 0;
+    if (jl <= P.ny) {
+        hn = (R)src.h[q + V];
+        hvn = (R)src.hv[q + V];
+    }
+#pragma unroll
+    for (int k = 0; k < V; k++) {
+        u[k] = 0;
+        v[k] = 0;
+        if (h[k] > K.hfilm) {
+            u[k] = PP::div(hu[k], h[k]);
+            v[k] = PP::div(hv[k], h[k]);
+        }
+    }
+    R smax = 0, s;
+#pragma unroll
+    for (int k = 0; k < V; k++) {
+        const int j = j0 + k;
+        if (j > P.ny) break;
+        const R c = PP::sqrtp(g[k] * h[k]);
+        /* x face i+1/2 */
+        if (below) {
+            const R ur = hd[k] > K.hfilm ? PP::div(hud[k], hd[k]) : R(0);
+            s = hll_speed<PP>(h[k], hd[k], u[k], ur, g[k], c, K.hfilm);
+        } else {
+            s = hll_speed<PP>(h[k], h[k], u[k], P.bndry[2] == 1 ? -u[k] : u[k], g[k], c, K.hfilm);
+        }
+        smax = (s > smax) ? s : smax;
+        /* y face j+1/2 */
+        R hr, vr;
+        if (j < P.ny) {
+            if (k + 1 < V) {
+                hr = h[k + 1];
+                vr = v[k + 1];
+            } else {
+                hr = hn;
+                vr = hn > K.hfilm ? PP::div(hvn, hn) : R(0);
+            }
+        } else if (P.inflow) {
+            hr = (R)(RS)inh;
+            vr = inh > K.hfilm ? PP::div(inhv, inh) : R(0);
+        } else {
+            hr = h[k];
+            vr = P.bndry[3] == 1 ? -v[k] : v[k];
+        }
+        s = hll_speed<PP>(h[k], hr, v[k], vr, g[k], c, K.hfilm);
+        smax = (s > smax) ? s : smax;
+        /* the domain's faces 1/2 */
+        if (i == 1) {
+            s = hll_speed<PP>(h[k], h[k], P.bndry[0] == 1 ? -u[k] : u[k], u[k], g[k], c, K.hfilm);
+            smax = (s > smax) ? s : smax;
+        }
+        if (j == 1) {
+            s = hll_speed<PP>(h[k], h[k], P.bndry[1] == 1 ? -v[k] : v[k], v[k], g[k], c, K.hfilm);
+            smax = (s > smax) ? s : smax;
+        }
+    }
+    return smax;
+}
+
 /* block maximum of the threads' partial maxima (result valid in thread 0) */
 __device__ __forceinline__ double block_max(double v, double *red8)
 {
@@ -781,18 +890,31 @@ __global__ void __launch_bounds__(TILE_THREADS, PP::kWaveMinBlocks) k_wave_cells
     /* cells in i-major order, j contiguous; (i, j) advanced by the stride */
     /* the cells of the rows this context updates; a face belongs to the
      * row of its lower (left) cell, face 1/2 to row 1 */
-    const int64_t total = (int64_t)(P.own_hi - P.own_lo + 1) * P.ny;
+    R smax = 0;
     const int64_t stride = (int64_t)gridDim.x * blockDim.x;
     const int64_t c0 = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    const int si = (int)(stride / P.ny), sj = (int)(stride - (int64_t)si * P.ny);
-    int i = (int)(c0 / P.ny) + P.own_lo, j = (int)(c0 - (int64_t)(i - P.own_lo) * P.ny) + 1;
-    R smax = 0;
-    for (int64_t c = c0; c < total; c += stride) {
-        const R s = wave_cell<PP, RS>(P, src, i, j, (R)inh, (R)inhv, P.has_solid ? B.solid : nullptr);
-        smax = (s > smax) ? s : smax;
-        i += si;
-        j += sj;
-        if (j > P.ny) { j -= P.ny; i++; }
+    if (!P.has_solid) {
+        /* V cells per thread and 16-byte loads (the pass is bound by load latency) */
+        constexpr int V = Cols<RS>::pad;
+        const int nv = (P.ny + V - 1) / V;
+        const int64_t total = (int64_t)(P.own_hi - P.own_lo + 1) * nv;
+        for (int64_t c = c0; c < total; c += stride) {
+            const int r = (int)(c / nv);
+            const int i = r + P.own_lo, j0 = (int)(c - (int64_t)r * nv) * V + 1;
+            const R s = wave_vec<PP, RS>(P, src, i, j0, (R)inh, (R)inhv);
+            smax = (s > smax) ? s : smax;
+        }
+    } else {
+        const int64_t total = (int64_t)(P.own_hi - P.own_lo + 1) * P.ny;
+        const int si = (int)(stride / P.ny), sj = (int)(stride - (int64_t)si * P.ny);
+        int i = (int)(c0 / P.ny) + P.own_lo, j = (int)(c0 - (int64_t)(i - P.own_lo) * P.ny) + 1;
+        for (int64_t c = c0; c < total; c += stride) {
+            const R s = wave_cell<PP, RS>(P, src, i, j, (R)inh, (R)inhv, B.solid);
+            smax = (s > smax) ? s : smax;
+            i += si;
+            j += sj;
+            if (j > P.ny) { j -= P.ny; i++; }
+        }
     }
     const double m = block_max((double)smax, red8);
     if (threadIdx.x == 0) {
@@ -1003,11 +1125,19 @@ __device__ __forceinline__ void tile_cell(const DevParams &P, const SetV<RS> &sr
     const R SYf = -gy * h0v;
     const R gz = PP::div(g, PP::sqrtp(sx * sx + sy * sy + 1));
     const R slope = PP::sqrtp(sx * sx + sy * sy);
+    /* variable-density forcing (SWEHR.c:1283-1290).  Where the TOTSED
+     * difference is an exact zero the term is a zero times a finite
+     * quotient, and 0 - (+-0) = +0: the FP64 form keeps gamma = +0 without
+     * the division sequence when the ranges keep the quotient finite. */
     R gammax = 0, gammay = 0;
-    if (i > 1 && i < P.nx)
+    auto zero_gradient = [&](int a, int b) {
+        return PP::kKnownResults && (R)sTS[a] - (R)sTS[b] == 0 && fabs((rhos - rho0c) * gz * h0v * h0v) <= R(0x1p800) &&
+               2 * rho0c >= R(0x1p-100);
+    };
+    if (i > 1 && i < P.nx && !zero_gradient(so + RJ, so - RJ))
         gammax -= PP::div((rhos - rho0c) * gz * h0v * h0v, 2 * rho0c) * half * K.oneoverdx
                   * ((R)sTS[so + RJ] - (R)sTS[so - RJ]);
-    if (j > 1 && j < P.ny)
+    if (j > 1 && j < P.ny && !zero_gradient(so + 1, so - 1))
         gammay -= PP::div((rhos - rho0c) * gz * h0v * h0v, 2 * rho0c) * half * K.oneoverdx
                   * ((R)sTS[so + 1] - (R)sTS[so - 1]);
     /* slope stability: provable "no failure" first, exact test otherwise */
