@@ -66,6 +66,7 @@ inline namespace SWEHR_TILE_NS {
 struct PolicyF64 {
     typedef double R;
     static constexpr int kMinBlocks = 2;      /* CTAs per SM the update kernel is register-budgeted for */
+    static constexpr int kBatchMinBlocks = 2; /* ... and the batched update kernel */
     /* the class loop of the cell update kept rolled: its unrolled body (eight
      * inline exp and division sequences) costs more in instruction fetch
      * than unrolling gains (measured: update -4 % rolled) */
@@ -157,6 +158,11 @@ struct PolicyF64 {
 struct PolicyF32 {
     typedef float R;
     static constexpr int kMinBlocks = 3;
+    /* the batched update reads its scenario's parameters from shared memory,
+     * not the constant bank, and needs more registers: at 3 CTAs per SM it
+     * spilled ~260 B per thread; at 2 (128 registers) the 256-scenario
+     * ensemble steps 1.2 % faster */
+    static constexpr int kBatchMinBlocks = 2;
     /* unrolled: 17 % faster than rolled with the class count exact */
     static constexpr bool kRollClasses = false;
     static constexpr int kWaveMinBlocks = 5;      /* 48 registers: four cells per thread without spills */
@@ -1829,7 +1835,7 @@ __global__ void __launch_bounds__(TILE_THREADS) k_wave_batch(const BatchHdr<RS> 
 /* Batched update pass, with the same per-scenario runs: budget accumulators
  * carry across a run and are summed, counted and folded once per run. */
 template <class PP, class RS, int MAXS, bool BUDGET, bool STAGE_M, int NS>
-__global__ void __launch_bounds__(TILE_THREADS, PP::kMinBlocks) k_update_batch(const BatchHdr<RS> *__restrict__ hdr)
+__global__ void __launch_bounds__(TILE_THREADS, PP::kBatchMinBlocks) k_update_batch(const BatchHdr<RS> *__restrict__ hdr)
 {
     typedef typename PP::R R;
     extern __shared__ __align__(128) unsigned char smb[];

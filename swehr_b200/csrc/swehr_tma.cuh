@@ -1,12 +1,12 @@
 /*
  * swehr_tma.cuh -- tile loads through the tensor memory accelerator for the
- * plain FP64 update kernel of one domain.
+ * update kernel of one domain (both forms).
  *
  * The staging of a tile (its halo planes, the two topography windows and
  * the cell planes, see swehr_tile.cuh) is a handful of rectangular boxes of
  * HBM planes.  With tensor maps of those planes one thread issues one
- * cp.async.bulk.tensor per box instead of every thread issuing pair copies
- * with its own address arithmetic; the copies complete on a shared-memory
+ * cp.async.bulk.tensor per box instead of every thread issuing 16-byte
+ * copies with its own address arithmetic; the copies complete on a shared-memory
  * mbarrier that carries the byte count, and parts of a box outside the grid
  * arrive as zeros (no cell reads them: ghost cells take their source cell's
  * values).  Loads only, from this GPU's own memory, no cluster multicast.
