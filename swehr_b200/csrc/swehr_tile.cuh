@@ -10,7 +10,8 @@
  *              deposited mass M_k, dt/t and the budgets stay FP64.
  *
  * A CTA of 256 threads owns 8 x 32 cells (i x j, j contiguous in HBM) and
- * loops over tiles (persistent grid).  Per tile:
+ * loops over tiles (persistent grid) of the rows the context updates (all
+ * rows, or a slab's own rows: DevParams own_lo..own_hi).  Per tile:
  *   A. the tile plus a one-cell halo (10 x 34 cells, ghosts resolved per
  *      SWEHR.c:816-1035) is staged in shared memory: h, the velocities
  *      u = hu/h and v = hv/h (0 when dry, SWEHR.c:333-352), the previous
