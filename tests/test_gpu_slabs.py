@@ -52,3 +52,11 @@ def test_slabs_match_whole_domain_under_a_moving_storm():
     # the storm's rain depends on each cell's global row (the slab's row offset)
     case = W.storm_domain(nx=48, ny=40, dx=1.0, seed=4, steps=200)
     _compare(case, 3, 200, FP64)
+
+
+@pytest.mark.parametrize("precision", [FP64, MIXED])
+def test_two_row_slabs(precision):
+    # the thinnest split: every slab owns two rows, so each halo is a whole
+    # neighbour slab, and the first and last slabs hold the domain's boundary rows
+    case = W.tiny_case(nx=8, ny=9, S=3, seed=5, bndry=(0, 1, 1, 1), inflow=1, rain_mmh=300.0, tend=60.0)
+    _compare(case, 4, 150, precision)
