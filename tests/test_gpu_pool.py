@@ -194,3 +194,15 @@ def test_pool_step_limit_and_cfl_error():
     with Simulation(c1) as s:
         pr = s.advance()
         assert pr.steps == pb.steps and s.status == 1
+
+
+def test_pool_exact_class_count_kernels():
+    """A pool whose running scenarios all have 7 (or all 10) classes steps them
+    with the batched kernel built for exactly that count; every scenario still
+    equals its single-domain run bit for bit."""
+    for S in (7, 10):
+        cases = [W.tiny_case(nx=20 + 3 * k, ny=15 + k, S=S, seed=60 + k, bndry=(0, 1, 1, 1), inflow=k % 2,
+                             rain_mmh=200.0, tend=40.0) for k in range(3)]
+        alone = [_alone(c, FP64) for c in cases]
+        got = _pool_all(cases, FP64, max_classes=16)
+        _check_same(got, alone, f"exact {S} classes")
